@@ -1,0 +1,413 @@
+"""Benchmark of the B200-native CSR product C = A·B.
+
+Workload (one step = one full product, symbolic + numeric, on one batch):
+C = A·A for the 27-point stencil on a 128^3 grid (n = 2,097,152,
+nnz(A) = 55,742,968, 1,489,355,288 intermediate products, nnz(C) =
+254,840,104), fp64 values, seeded synthetic data. With N GPUs (torchrun)
+the grid grows to 128 x 128 x (128 N) and rank r owns the z-slab of planes
+[128 r, 128 r + 128): its rows of A times the B rows they reference (its
+slab plus one halo plane each side, generated locally), so per-GPU work is
+fixed (weak scaling) and no collective touches the data path.
+
+value  = GFLOP/s (2 x intermediate products / time), inputs resident in HBM,
+         C written into preallocated buffers, whole job (sum over ranks of
+         the work / max over ranks of the time).
+e2e    = the same metric through the reference-facing entry point
+         nsp_spgemm_kernel_hash (C allocated inside with cudaMalloc, as in
+         the reference) with A copied host->device before and C copied
+         device->host after, every step.
+--impl reference: the CPU product (OpenMP Gustavson restating the
+         reference's semantics; the reference has no CPU implementation) on
+         all host cores, same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = 128
+SEED = 20261203
+METRIC = "SpGEMM GFLOP/s, C=A*A, 27-point stencil 128^3, fp64"
+WORKLOAD = "stencil27_128^3_AxA_fp64"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="nspb", choices=["nspb", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def local_problem(rank, world):
+    """This rank's A row block (global columns) and the B rows it needs, with
+    A's columns shifted to index them."""
+    import nsp_b200 as nb
+    nz = L * world
+    z0, z1 = L * rank, L * (rank + 1)
+    A = nb.gen.stencil_slab(L, L, nz, z0, z1, 27, SEED)
+    if world == 1:
+        return A, A
+    h0, h1 = max(z0 - 1, 0), min(z1 + 1, nz)
+    B = nb.gen.stencil_slab(L, L, nz, h0, h1, 27, SEED)
+    A.col = (A.col - h0 * L * L).astype(np.int32)
+    A.ncols = B.nrows
+    return A, B
+
+
+def alg_bytes(A, B, nnz_c):
+    """Every input read once and C written once (rowptr int32, col int32,
+    val fp64)."""
+    return (4 * (A.nrows + 1) + 12 * A.nnz + 4 * (B.nrows + 1) + 12 * B.nnz
+            + 4 * (A.nrows + 1) + 12 * nnz_c)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/roofline_traffic.txt: 'kernel: bytes' lines)."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith(kernel + ":"):
+                return float(line.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_product_rate(A, B, rows, threads):
+    """GFLOP/s of the CPU oracle on rows [0, rows) of A·B (one timed run
+    after one warm-up)."""
+    import oracle
+    ip, _ = oracle.intprod(A, B, threads)
+    flops = 2.0 * float(ip[:rows].sum())
+    oracle.spgemm_rows(A, B, 0, min(rows, 2000), threads)
+    t0 = time.perf_counter()
+    oracle.spgemm_rows(A, B, 0, rows, threads)
+    dt = time.perf_counter() - t0
+    return flops / dt / 1e9, dt
+
+
+def sample_rows(A, B, threads, budget_s=8.0):
+    """Largest leading row block the CPU finishes in about budget_s."""
+    import oracle
+    probe = min(A.nrows, 65536)
+    _, dt = cpu_product_rate(A, B, probe, threads)
+    rows = int(probe * budget_s / max(dt, 1e-6))
+    return max(1, min(A.nrows, rows))
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the oracle (OpenMP Gustavson) on all host cores."""
+    if rank != 0:
+        return
+    import oracle
+    A, B = local_problem(0, 1)
+    threads = os.cpu_count() or 1
+    rows = sample_rows(A, B, threads, budget_s=max(2.0, 120.0 / max(args.steps + args.warmup, 1)))
+    ip, _ = oracle.intprod(A, B, threads)
+    flops = 2.0 * float(ip[:rows].sum())
+    for _ in range(args.warmup):
+        oracle.spgemm_rows(A, B, 0, rows, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.spgemm_rows(A, B, 0, rows, threads)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    v = flops / t / 1e9
+    sample = f"rows [0,{rows}) of {A.nrows} ({rows / A.nrows:.1%}), {flops / 2:.3e} products"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic (seeded 27-point stencil, seed {SEED})",
+        "config": {"workload": WORKLOAD, "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import ctypes as C
+    import torch
+    import nsp_b200 as nb
+    from nsp_b200 import _lib
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.SUM)
+        return float(t.item())
+
+    Ah, Bh = local_problem(rank, world)
+    dA = Ah.to_device(dev)
+    dB = dA if Bh is Ah else Bh.to_device(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # size C once (symbolic), preallocate it, then time full products into it
+    C0, st0 = nb.spgemm(dA, dB, return_stats=True)
+    nnz_c = st0["nnz"]
+    intprod = st0["intprod"]
+    del C0
+    out = nb.DeviceCSR(dA.nrows, dB.ncols,
+                       torch.empty(dA.nrows + 1, dtype=torch.int32, device=dev),
+                       torch.empty(nnz_c, dtype=torch.int32, device=dev),
+                       torch.empty(nnz_c, dtype=torch.float64, device=dev))
+    a_in, b_in = dA.as_in(), dB.as_in()
+    c_out = _lib.CsrOut()
+    c_out.rowptr, c_out.col, c_out.val = (out.rowptr.data_ptr(), out.col.data_ptr(),
+                                          out.val.data_ptr())
+    c_out.capacity = nnz_c
+    opts = nb.make_opts(check_errors=False, stream=stream)
+    opts.timing = 1
+    stats = _lib.Stats()
+
+    def step():
+        _lib.check(nb.lib.nspb_spgemm(C.byref(a_in), C.byref(b_in), C.byref(c_out),
+                                      C.byref(opts), C.byref(stats)), "nspb_spgemm")
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phase = {"ms_rowinfo": 0.0, "ms_symbolic": 0.0, "ms_scan": 0.0, "ms_numeric": 0.0}
+    launches = 0
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        for k in phase:
+            phase[k] += getattr(stats, k)
+        launches += stats.launches
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    ms_local = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms_local)
+    flops_all = sum_over_ranks(2.0 * intprod)
+    value = flops_all / (ms * 1e-3) / 1e9
+    for k in phase:
+        phase[k] /= args.steps
+
+    # correctness guard on the measured configuration: a final checked call
+    opts.check_errors = 1
+    step()
+    torch.cuda.synchronize(dev)
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = peaks()
+    dominant = "numeric" if phase["ms_numeric"] >= phase["ms_symbolic"] else "symbolic"
+    if dominant == "numeric":
+        kbytes = alg_bytes(Ah, Bh, nnz_c)
+        kms = phase["ms_numeric"]
+        kname = "k_num_group"
+    else:
+        kbytes = 4 * (Ah.nrows + 1) + 4 * Ah.nnz + 4 * (Bh.nrows + 1) + 4 * Bh.nnz + 4 * Ah.nrows
+        kms = phase["ms_symbolic"]
+        kname = "k_sym_group"
+    achieved = kbytes / (kms * 1e-3) / 1e9 if kms > 0 else 0.0
+    traffic = profiled_traffic(kname)
+
+    # ---- end to end through the reference-facing entry point, host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        hA = [torch.from_numpy(x).pin_memory() for x in (Ah.rowptr, Ah.col, Ah.val)]
+        hB = hA if Bh is Ah else [torch.from_numpy(x).pin_memory()
+                                  for x in (Bh.rowptr, Bh.col, Bh.val)]
+        dA2 = [torch.empty_like(x, device=dev) for x in hA]
+        dB2 = dA2 if Bh is Ah else [torch.empty_like(x, device=dev) for x in hB]
+        hC = [torch.empty(dA.nrows + 1, dtype=torch.int32).pin_memory(),
+              torch.empty(nnz_c, dtype=torch.int32).pin_memory(),
+              torch.empty(nnz_c, dtype=torch.float64).pin_memory()]
+        h2d = sum(x.numel() * x.element_size() for x in hA)
+        if Bh is not Ah:
+            h2d += sum(x.numel() * x.element_size() for x in hB)
+        d2h = sum(x.numel() * x.element_size() for x in hC)
+
+        def e2e_step():
+            for d, h in zip(dA2, hA):
+                d.copy_(h, non_blocking=True)
+            if Bh is not Ah:
+                for d, h in zip(dB2, hB):
+                    d.copy_(h, non_blocking=True)
+            sa, sb, sc = _lib.SfCSR(), _lib.SfCSR(), _lib.SfCSR()
+            for s, m, d in ((sa, Ah, dA2), (sb, Bh, dB2)):
+                s.M, s.N, s.nnz = m.nrows, m.ncols, m.nnz
+                s.d_rpt, s.d_col, s.d_val = d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr()
+            nb.nsp_spgemm_kernel_hash(sa, sb, sc)
+            # C's arrays were cudaMalloc'ed by the call: read them back, then
+            # free them (the tensors own them through nspb_free)
+            res = (nb.adopt(sc.d_rpt, sc.M + 1, "int32"), nb.adopt(sc.d_col, sc.nnz, "int32"),
+                   nb.adopt(sc.d_val, sc.nnz, "float64"))
+            for h, d in zip(hC, res):
+                h.copy_(d)
+            del res
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.e2e_steps)
+        e2e = {"value": flops_all / (e2e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e2e_ms, "steps": args.e2e_steps,
+               "entry": "nsp_spgemm_kernel_hash (sfCSR), C cudaMalloc'ed inside"}
+
+    # ---- CPU baseline (rank 0 at N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rows = sample_rows(Ah, Bh, threads, budget_s=10.0)
+        v, dt = cpu_product_rate(Ah, Bh, rows, threads)
+        cpu = {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+               "sample": f"rows [0,{rows}) of {Ah.nrows} ({rows / Ah.nrows:.1%}) of the same "
+                         f"product, {dt:.1f} s, OpenMP Gustavson oracle"}
+
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        gbs = alg_bytes(Ah, Bh, nnz_c) * world / (ms * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic (seeded 27-point stencil, seed {SEED})",
+            "config": {"workload": WORKLOAD, "grid": [L, L, L * world], "n_rows_per_gpu": dA.nrows,
+                       "nnz_A_per_gpu": dA.nnz, "intprod_per_gpu": intprod,
+                       "nnz_C_per_gpu": nnz_c,
+                       "l2": "inputs (669 MB) and C (3.06 GB) exceed the 126 MB L2; no flush",
+                       "parallelism": "row z-slabs per GPU, halo planes generated locally, "
+                                      "no collective"},
+            "effective_gbs": gbs,
+            "phases_ms": phase,
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes": kbytes,
+                         "ms_per_launch": kms},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

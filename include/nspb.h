@@ -1,0 +1,223 @@
+/*
+ * nspb.h — C ABI of the B200-native CSR sparse matrix product C = A·B.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes and
+ * returns an int status (0 = success, negative = nspb_status). Device
+ * pointers are CUDA device addresses on the current device; streams are
+ * passed as `void*` (a cudaStream_t, NULL = the legacy default stream).
+ *
+ * Reference interfaces replaced (file:line in amavliut/nsp):
+ *   nspb_spgemm            <- nsp_spgemm_kernel_hash   nsp/inc/nsp.h:105,
+ *                             nsp/src/nsp.cu:2448-2488 (one call, C allocated
+ *                             inside, row_ptr/col/val device arrays)
+ *   nspb_spgemm_symbolic   <- nsp_set_max_bin + nsp_set_row_nnz
+ *                             nsp/src/nsp.cu:417-471, 921-1130 (row counts and
+ *                             the exclusive scan to row_ptr)
+ *   nspb_spgemm_numeric    <- nsp_set_min_bin + nsp_calculate_value_col_bin
+ *                             nsp/src/nsp.cu:1241-1300, 2178-2440
+ *   nspb_intprod           <- nsp_set_intprod_num      nsp/src/nsp.cu:306-320
+ *   nspb_getmct            <- getmct                   src/getmct.cu:41-92
+ *   nspb_compactcol        <- compactcol / cuCompactor src/compactcol.cu:160-163
+ *   nspb_shrink_col        <- get_shrinked_col / apply_mask_permut_GPU_noSideEffects
+ *                             src/spspmpi.cu:58-104, 106-182
+ *   nspb_spgemm_batched    <- no single reference entry point: replaces a host
+ *                             loop of nsp_spgemm_kernel_hash calls (one per
+ *                             Galerkin product), src/spspmpi.cu:266-313
+ *   nspb_spgemm_rowblocked <- nsparseMGPU_version1's shrink + local product,
+ *                             src/spspmpi.cu:906-935, run per row block on one GPU
+ *
+ * C++ drop-in shims with the reference's own signatures (sfCSR, CSR,
+ * nsparseMGPU_version0/1) are declared in nspb_compat.h.
+ */
+#ifndef NSPB_H
+#define NSPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+typedef enum {
+  NSPB_OK = 0,
+  NSPB_ERR_INVALID = -1,   /* null pointer, negative size, dimension mismatch   */
+  NSPB_ERR_OVERFLOW = -2,  /* nnz(C) or a row count does not fit int32          */
+  NSPB_ERR_ALLOC = -3,     /* device or pinned-host allocation failed           */
+  NSPB_ERR_CUDA = -4,      /* a CUDA runtime call failed (see nspb_last_cuda_error) */
+  NSPB_ERR_DEVICE = -5,    /* a kernel raised its error word (bounded probe or
+                              bounded wait exhausted); results are invalid      */
+  NSPB_ERR_NO_DEVICE = -6, /* no CUDA device visible                            */
+  NSPB_ERR_UNSUPPORTED = -7,
+  NSPB_ERR_CAPACITY = -8   /* a size exceeds a fixed capacity of the call       */
+} nspb_status;
+
+/* value types */
+enum { NSPB_F64 = 0, NSPB_F32 = 1 };
+
+/* precision modes of the product */
+enum {
+  NSPB_PREC_FP64 = 0,      /* fp64 inputs, fp64 accumulation (the drop-in)       */
+  NSPB_PREC_FP32_COMP = 1  /* fp32 inputs, error-free fp32 products and two-sum
+                              compensated accumulation, fp64 output; rows whose
+                              running error bound exceeds opts.comp_tol are
+                              re-accumulated in fp64                            */
+};
+
+/* A CSR matrix on the device. rowptr has nrows+1 entries, 0-based, int32.   */
+typedef struct {
+  int32_t nrows;
+  int32_t ncols;
+  int64_t nnz;
+  const int32_t *rowptr;
+  const int32_t *col;
+  const void *val;       /* nnz values of val_type                          */
+  int32_t val_type;      /* NSPB_F64 or NSPB_F32                            */
+  int32_t _pad;
+} nspb_csr_in;
+
+/* Output CSR. If `col`/`val` are NULL on entry, the call allocates them with
+ * cudaMalloc (release with cudaFree or nspb_free). If they are non-NULL,
+ * `capacity` must hold their length in entries; the call fails with
+ * NSPB_ERR_CAPACITY when nnz(C) exceeds it. `rowptr` follows the same rule
+ * (nrows+1 entries). val is always fp64.                                    */
+typedef struct {
+  int32_t nrows;
+  int32_t ncols;
+  int64_t nnz;
+  int32_t *rowptr;
+  int32_t *col;
+  double *val;
+  int64_t capacity;
+} nspb_csr_out;
+
+typedef struct {
+  int32_t precision;     /* NSPB_PREC_*                                      */
+  int32_t assume_sorted; /* 1: caller guarantees B rows strictly increasing
+                            (skips the B check pass)                         */
+  int32_t check_errors;  /* 1: synchronise at the end and report device
+                            error words                                      */
+  int32_t group_lanes;   /* 0 = auto; else 8, 16 or 32 lanes per row group    */
+  int32_t timing;        /* 1: record CUDA events around each phase (stats)  */
+  int32_t _pad;
+  double comp_tol;       /* FP32_COMP: relative error bound per row before the
+                            row is redone in fp64 (default 1e-12 when 0)      */
+  void *stream;          /* cudaStream_t                                     */
+} nspb_opts;
+
+/* Per-call figures (all optional; pass NULL).                               */
+typedef struct {
+  int64_t intprod;       /* sum_i sum_{k in A(i,:)} nnz(B(k,:))              */
+  int64_t nnz;           /* nnz(C)                                           */
+  int32_t sym_bins[16];  /* rows per symbolic bin                            */
+  int32_t num_bins[16];  /* rows per numeric bin                             */
+  int32_t rows_redone;   /* FP32_COMP: rows re-accumulated in fp64           */
+  int32_t b_sorted;      /* 1 if B rows were found strictly increasing       */
+  double max_row_err;    /* FP32_COMP: largest per-row error bound (relative) */
+  int32_t launches;      /* kernels this call launched                       */
+  float ms_rowinfo;      /* opts.timing: B check + row counts + bins         */
+  float ms_symbolic;     /* opts.timing: permutation + symbolic kernels      */
+  float ms_scan;         /* opts.timing: row_ptr scan                        */
+  float ms_numeric;      /* opts.timing: permutation + numeric kernels       */
+  float _pad;
+} nspb_stats;
+
+/* ---- library ------------------------------------------------------------ */
+const char *nspb_version(void);
+const char *nspb_strerror(int status);
+int nspb_last_cuda_error(void);          /* cudaError_t of the last failure  */
+void nspb_default_opts(nspb_opts *opts);
+int nspb_free(void *device_ptr);         /* cudaFree                         */
+int nspb_device_sm_count(int *sms);
+
+/* ---- the product ---------------------------------------------------------- */
+/* C = A·B. One call: counts, allocates C (unless provided), fills it. On
+ * return C->rowptr/col/val are complete in stream order on opts->stream; the
+ * call itself synchronises twice on the host (bin sizes; nnz(C)).           */
+int nspb_spgemm(const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
+                const nspb_opts *opts, nspb_stats *stats);
+
+/* Two-call form. symbolic writes C->rowptr (allocating it when NULL) and sets
+ * C->nnz; numeric fills C->col/C->val (allocating when NULL). The structure
+ * of A and B must not change between the two calls.                         */
+int nspb_spgemm_symbolic(const nspb_csr_in *A, const nspb_csr_in *B,
+                         nspb_csr_out *C, const nspb_opts *opts,
+                         nspb_stats *stats);
+int nspb_spgemm_numeric(const nspb_csr_in *A, const nspb_csr_in *B,
+                        nspb_csr_out *C, const nspb_opts *opts,
+                        nspb_stats *stats);
+
+/* Per-row intermediate-product counts (device out, int64[nrows]) and their
+ * total (host out).                                                          */
+int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip,
+                 int64_t *total, void *stream);
+
+/* ---- batched products ------------------------------------------------------ */
+/* `count` independent products C[i] = A[i]·B[i] run through one persistent
+ * kernel per phase with a global row work queue across all products. Output
+ * arrays are allocated per product with one cudaMalloc each (caller frees).  */
+int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
+                        nspb_csr_out *C, const nspb_opts *opts,
+                        nspb_stats *stats);
+
+/* ---- column remap (compactcol / getmct) ------------------------------------ */
+/* Sorted unique column indices of col[0..nnz) that fall outside [first,last]
+ * (when first > last: all columns). d_out must hold nnz entries; *nout is
+ * the number written.                                                        */
+int nspb_getmct(const int32_t *d_col, int64_t nnz, int32_t first, int32_t last,
+                int32_t *d_out, int64_t *nout, void *stream);
+/* Stream compaction: d_out[j] = d_in[i] for the i with pred(d_in[i]) in
+ * order, pred(x) = (x < lo || x > hi). *nout = count.                        */
+int nspb_compactcol(const int32_t *d_in, int64_t n, int32_t lo, int32_t hi,
+                    int32_t *d_out, int64_t *nout, void *stream);
+/* Remap each column of d_col to its position in the sorted list d_cols
+ * (binary search); columns absent from the list map to -1.                  */
+int nspb_shrink_col(const int32_t *d_col, int64_t nnz, const int32_t *d_cols,
+                    int64_t ncols, int32_t *d_out, void *stream);
+
+/* Row-blocked product for C larger than a device budget: A is split into
+ * contiguous row blocks whose C fits `budget_bytes`; per block the B rows it
+ * references are gathered (getmct + shrink), the block product runs, and the
+ * block of C is copied to the HOST arrays h_rowptr/h_col/h_val (caller sizes
+ * them from nspb_spgemm_symbolic or an upper bound `h_capacity`).            */
+int nspb_spgemm_rowblocked(const nspb_csr_in *A, const nspb_csr_in *B,
+                           int64_t budget_bytes, int32_t *h_rowptr,
+                           int32_t *h_col, double *h_val, int64_t h_capacity,
+                           int64_t *nnz_out, int32_t *nblocks_out,
+                           const nspb_opts *opts);
+
+/* ---- seeded input generators (host memory) --------------------------------- */
+/* Each fills rowptr[nrows+1] and returns nnz (>=0) or a negative status; col
+ * and val are filled when non-NULL. Values depend only on (seed, row, slot),
+ * never on the thread count.                                                 */
+/* 3-D stencil on nx*ny*nz, npts = 7 (diag 6, off -1) or 27 (off uniform[-1,1],
+ * diag = sum|off| + 1). fp32_values rounds every value to float first.       */
+int64_t nspb_gen_stencil(int32_t nx, int32_t ny, int32_t nz, int32_t npts,
+                         uint64_t seed, int32_t fp32_values, int32_t *rowptr,
+                         int32_t *col, double *val);
+/* Rows of the z-planes [z0, z1) of the same stencil (global column ids):
+ * the row block one GPU owns when the grid is split into z-slabs.           */
+int64_t nspb_gen_stencil_slab(int32_t nx, int32_t ny, int32_t nz, int32_t z0,
+                              int32_t z1, int32_t npts, uint64_t seed,
+                              int32_t fp32_values, int32_t *rowptr,
+                              int32_t *col, double *val);
+/* Power-law rows: degree ~ truncated Pareto(alpha) with its lower bound
+ * solved so the mean degree is `mean_deg`, capped at max_deg; columns uniform
+ * without duplicates, sorted; values uniform[-1,1].                         */
+int64_t nspb_gen_powerlaw(int32_t nrows, int32_t ncols, double alpha,
+                          double mean_deg, int32_t max_deg, uint64_t seed,
+                          int32_t fp32_values, int32_t *rowptr, int32_t *col,
+                          double *val);
+/* Uniform random rows: degree uniform in [dmin,dmax] (clamped to ncols),
+ * columns uniform without duplicates, sorted; values uniform[-1,1].          */
+int64_t nspb_gen_random(int32_t nrows, int32_t ncols, int32_t dmin,
+                        int32_t dmax, uint64_t seed, int32_t fp32_values,
+                        int32_t *rowptr, int32_t *col, double *val);
+/* Lower bound x_min of the truncated Pareto used by nspb_gen_powerlaw.       */
+double nspb_powerlaw_xmin(double alpha, double mean_deg, int32_t max_deg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NSPB_H */

@@ -1,0 +1,160 @@
+"""nsp_b200 — B200-native (sm_100a) CSR sparse matrix product C = A·B.
+
+The product runs in libnspb.so (hand-written CUDA kernels behind the C ABI
+of include/nspb.h). This package is the Python glue used by the tests and
+the benchmark: ctypes bindings, CSR containers and the seeded generators.
+
+Entry points mirroring the reference (amavliut/nsp):
+  nsp_spgemm_kernel_hash(a, b, c)   nsp/inc/nsp.h:105 on sfCSR structs
+  nsparseMGPU_version1(A, B)        src/spspmpi.h:31 (one GPU) -> (C, loc_time)
+  spgemm(A, B, ...)                 the C-ABI one-call product
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import gen
+from ._lib import (F32, F64, PREC_FP32_COMP, PREC_FP64, CsrIn, CsrOut, NspbError, Opts,
+                   SfCSR, Stats, check, lib)
+from .csr import DeviceCSR, HostCSR, adopt
+
+__all__ = ["spgemm", "spgemm_symbolic", "spgemm_numeric", "intprod", "nsp_spgemm_kernel_hash",
+           "nsparseMGPU_version1", "DeviceCSR", "HostCSR", "gen", "NspbError", "lib",
+           "make_opts", "stats_dict"]
+
+
+def _stream_ptr(stream):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group_lanes=0,
+              comp_tol=1e-12, stream=None) -> Opts:
+    o = Opts()
+    lib.nspb_default_opts(C.byref(o))
+    o.precision = precision
+    o.assume_sorted = int(assume_sorted)
+    o.check_errors = int(check_errors)
+    o.group_lanes = int(group_lanes)
+    o.comp_tol = float(comp_tol)
+    o.stream = _stream_ptr(stream)
+    return o
+
+
+def stats_dict(s: Stats) -> dict:
+    return {"intprod": s.intprod, "nnz": s.nnz, "sym_bins": list(s.sym_bins)[:12],
+            "num_bins": list(s.num_bins)[:10], "rows_redone": s.rows_redone,
+            "b_sorted": s.b_sorted, "max_row_err": s.max_row_err}
+
+
+def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,
+           stream=None, check_errors: bool = True, assume_sorted: bool = False,
+           group_lanes: int = 0, comp_tol: float = 1e-12, return_stats: bool = False):
+    """C = A·B on the current CUDA device through nspb_spgemm.
+
+    With `out` given, its tensors are used as C's arrays (capacity = their
+    length); otherwise the library allocates C (freed with the tensors)."""
+    import torch
+    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream)
+    a, b = A.as_in(), B.as_in()
+    c = CsrOut()
+    if out is not None:
+        c.rowptr = out.rowptr.data_ptr()
+        c.col = out.col.data_ptr()
+        c.val = out.val.data_ptr()
+        c.capacity = min(out.col.numel(), out.val.numel())
+    st = Stats()
+    check(lib.nspb_spgemm(C.byref(a), C.byref(b), C.byref(c), C.byref(o), C.byref(st)),
+          "nspb_spgemm")
+    if out is not None:
+        res = DeviceCSR(A.nrows, B.ncols, out.rowptr, out.col[:c.nnz], out.val[:c.nnz])
+    else:
+        res = DeviceCSR(A.nrows, B.ncols, adopt(c.rowptr, A.nrows + 1, "int32"),
+                        adopt(c.col, c.nnz, "int32"), adopt(c.val, c.nnz, "float64"))
+    return (res, stats_dict(st)) if return_stats else res
+
+
+def spgemm_symbolic(A: DeviceCSR, B: DeviceCSR, stream=None, assume_sorted=False):
+    """Two-call form, step 1: returns (rowptr tensor, nnz)."""
+    import torch
+    o = make_opts(PREC_FP64, assume_sorted, True, 0, 1e-12, stream)
+    if A.val.dtype == torch.float32:
+        o.precision = PREC_FP32_COMP
+    a, b = A.as_in(), B.as_in()
+    rowptr = torch.empty(A.nrows + 1, dtype=torch.int32, device=A.rowptr.device)
+    c = CsrOut()
+    c.rowptr = rowptr.data_ptr()
+    check(lib.nspb_spgemm_symbolic(C.byref(a), C.byref(b), C.byref(c), C.byref(o), None),
+          "nspb_spgemm_symbolic")
+    return rowptr, int(c.nnz)
+
+
+def spgemm_numeric(A: DeviceCSR, B: DeviceCSR, rowptr, nnz: int, precision="fp64",
+                   stream=None, assume_sorted=False) -> DeviceCSR:
+    """Two-call form, step 2: fills col/val for the given rowptr."""
+    import torch
+    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    o = make_opts(prec, assume_sorted, True, 0, 1e-12, stream)
+    a, b = A.as_in(), B.as_in()
+    col = torch.empty(max(nnz, 1), dtype=torch.int32, device=rowptr.device)
+    val = torch.empty(max(nnz, 1), dtype=torch.float64, device=rowptr.device)
+    c = CsrOut()
+    c.nnz = nnz
+    c.rowptr = rowptr.data_ptr()
+    c.col = col.data_ptr()
+    c.val = val.data_ptr()
+    c.capacity = max(nnz, 1)
+    check(lib.nspb_spgemm_numeric(C.byref(a), C.byref(b), C.byref(c), C.byref(o), None),
+          "nspb_spgemm_numeric")
+    return DeviceCSR(A.nrows, B.ncols, rowptr, col[:nnz], val[:nnz])
+
+
+def intprod(A: DeviceCSR, B: DeviceCSR, stream=None):
+    """Per-row intermediate-product counts (int64 tensor) and their total."""
+    import torch
+    row_ip = torch.empty(max(A.nrows, 1), dtype=torch.int64, device=A.rowptr.device)
+    tot = C.c_int64(0)
+    a, b = A.as_in(), B.as_in()
+    check(lib.nspb_intprod(C.byref(a), C.byref(b), C.c_void_p(row_ip.data_ptr()),
+                           C.byref(tot), _stream_ptr(stream)), "nspb_intprod")
+    return row_ip[:A.nrows], int(tot.value)
+
+
+def sfcsr_of(m: DeviceCSR) -> SfCSR:
+    """sfCSR view of a device CSR (nsp/inc/nsp.h:57-70)."""
+    s = SfCSR()
+    s.M = m.nrows
+    s.N = m.ncols
+    s.nnz = m.nnz
+    s.d_rpt = m.rowptr.data_ptr()
+    s.d_col = m.col.data_ptr() if m.nnz else None
+    s.d_val = m.val.data_ptr() if m.nnz else None
+    return s
+
+
+def nsp_spgemm_kernel_hash(a: SfCSR, b: SfCSR, c: SfCSR) -> None:
+    """The reference entry point (nsp/inc/nsp.h:105): fills c->M, N, nnz and
+    cudaMalloc'ed c->d_rpt/d_col/d_val. Raises NspbError on failure (the C++
+    shim of the same name exits the process instead, like the reference)."""
+    check(lib.nspb_nsp_spgemm_kernel_hash(C.byref(a), C.byref(b), C.byref(c)),
+          "nsp_spgemm_kernel_hash")
+
+
+def nsparseMGPU_version1(A: DeviceCSR, B: DeviceCSR):
+    """One-GPU nsparseMGPU_version1 (src/spspmpi.cu:371, nprocs == 1 path):
+    returns (C, loc_time) with loc_time the wall seconds of the product
+    bracketed by device synchronisation (src/spspmpi.cu:288-305)."""
+    import time
+    import torch
+    a, b, c = sfcsr_of(A), sfcsr_of(B), SfCSR()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nsp_spgemm_kernel_hash(a, b, c)
+    torch.cuda.synchronize()
+    loc = time.perf_counter() - t0
+    res = DeviceCSR(c.M, c.N, adopt(c.d_rpt, c.M + 1, "int32"), adopt(c.d_col, c.nnz, "int32"),
+                    adopt(c.d_val, c.nnz, "float64"))
+    return res, loc

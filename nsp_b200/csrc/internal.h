@@ -1,0 +1,84 @@
+// Host-side interfaces between the orchestration (spgemm.cu) and the kernel
+// translation units. Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/nspb.h"
+
+namespace nspb {
+
+struct DevInfo {
+  int device = -1;
+  int sms = 0;
+  int smem_optin = 0;  // max dynamic shared memory per block (opt-in)
+};
+// Properties of the current device (cached per device).
+const DevInfo &dev_info();
+
+// Internal device view of a CSR operand (fp64 values unless noted).
+struct CsrDev {
+  int nrows = 0, ncols = 0;
+  int64_t nnz = 0;
+  const int *rpt = nullptr;
+  const int *col = nullptr;
+  const double *val = nullptr;
+  const float *val32 = nullptr;  // fp32 operands (FP32_COMP mode)
+};
+
+// Flag bits written by launch_check_sorted.
+enum : int { B_UNSORTED = 1 };
+
+// ---- rowinfo.cu -----------------------------------------------------------------
+cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s);
+// row_nz[i] = min(intprod_i, ncols(B)); sym_counts[b] += rows of symbolic bin b
+// (rows with zero products are not binned); *total_ip += sum of intprod_i.
+// row_ip (optional) receives intprod_i as int64.
+cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
+                           int64_t *row_ip, int *sym_counts,
+                           unsigned long long *total_ip, cudaStream_t s);
+// Scatter rows into bin-contiguous order. kind 0: key = ub (symbolic bins),
+// kind 1: key = crpt[i+1]-crpt[i] (numeric bins). offsets: 16 bin starts.
+struct BinOffsets {
+  int v[16];
+};
+cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets,
+                        int *cursor, int *perm, cudaStream_t s);
+// Single-pass exclusive scan of row_nz into crpt[0..n] (crpt[n] = total) with
+// the numeric-bin histogram of the counts. Workspace: tile_state (zeroed,
+// scan_tiles(n) entries) and tile_ctr (zeroed).
+int scan_tiles(int n);
+cudaError_t launch_scan(const int *row_nz, int n, int *crpt, long long *total,
+                        unsigned long long *tile_state, int *tile_ctr,
+                        int *num_counts, int *err, cudaStream_t s);
+// Numeric-bin histogram from an existing row pointer.
+cudaError_t launch_num_hist(const int *crpt, int n, int *num_counts,
+                            cudaStream_t s);
+
+// ---- symbolic.cu ----------------------------------------------------------------
+cudaError_t launch_symbolic_bin(int bin, int lanes, const CsrDev &A,
+                                const CsrDev &B, const int *rows, int count,
+                                int *row_nz, int *err, cudaStream_t s);
+
+// ---- numeric.cu -----------------------------------------------------------------
+// owned: B rows hold no duplicate columns (deterministic plain accumulation).
+// b_sorted: B rows strictly increasing (long rows use binary search).
+cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
+                               const CsrDev &A, const CsrDev &B,
+                               const int *crpt, int *ccol, double *cval,
+                               const int *rows, int count, int *err,
+                               cudaStream_t s);
+
+// ---- fp32c.cu ---------------------------------------------------------------------
+// FP32 compensated numeric phase: fp32 inputs, error-free products and
+// two-sum accumulation, fp64 output, per-row relative error bound written to
+// row_err (bound relative to sum|a*b|). Rows flagged in redo get fp64 values.
+cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool b_sorted,
+                                    const CsrDev &A, const CsrDev &B,
+                                    const int *crpt, int *ccol, double *cval,
+                                    const int *rows, int count, double tol,
+                                    int *redo_rows, int *redo_count,
+                                    float *row_err, int *err, cudaStream_t s);
+
+}  // namespace nspb

@@ -1,0 +1,262 @@
+// Row analysis kernels: B-row order check, intermediate-product counts and
+// symbolic binning, bin permutation, and the single-pass row_ptr scan.
+//
+// Reference counterparts (amavliut/nsp):
+//   nsp_set_intprod_num  nsp/src/nsp.cu:306-320   (one thread per row)
+//   nsp_set_bin          nsp/src/nsp.cu:325-352   (10 global atomics per thread)
+//   nsp_set_row_perm     nsp/src/nsp.cu:356-411   (one global atomic per row)
+//   cub::DeviceScan::ExclusiveSum + D2H of nnz     nsp/src/nsp.cu:1124-1126
+//   nsp_set_bin_min / nsp_set_row_perm_min          nsp/src/nsp.cu:1137-1237
+// Here a row group of lanes reads each A row coalesced, bins are counted in
+// shared memory with one global atomic per bin per block, and the scan is a
+// single pass with decoupled look-back that also histograms the numeric bins.
+#include "common.cuh"
+#include "internal.h"
+
+namespace nspb {
+
+// ---- B row order --------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_check_sorted(const int *__restrict__ rpt, const int *__restrict__ col,
+                   int n, int *__restrict__ flags) {
+  const int row = (blockIdx.x * 256 + threadIdx.x) >> 3;
+  const int lane = threadIdx.x & 7;
+  int bad = 0;
+  if (row < n) {
+    const int s0 = rpt[row], s1 = rpt[row + 1];
+    for (int e = s0 + lane; e + 1 < s1; e += 8) bad |= (col[e] >= col[e + 1]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags, B_UNSORTED);
+}
+
+cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s) {
+  if (B.nrows <= 0) return cudaSuccess;
+  const int grid = (int)(((int64_t)B.nrows * 8 + 255) / 256);
+  k_check_sorted<<<grid, 256, 0, s>>>(B.rpt, B.col, B.nrows, flags);
+  return cudaGetLastError();
+}
+
+// ---- intermediate products and symbolic bins ---------------------------------
+template <int GA>
+__global__ void __launch_bounds__(256)
+    k_rowinfo(const int *__restrict__ arpt, const int *__restrict__ acol,
+              const int *__restrict__ brpt, int n, int ncols_b,
+              int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
+              int *__restrict__ sym_counts,
+              unsigned long long *__restrict__ total_ip) {
+  __shared__ int hist[kSymBins];
+  __shared__ unsigned long long s_total;
+  if (threadIdx.x < kSymBins) hist[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_total = 0ull;
+  __syncthreads();
+  auto tile = cg::tiled_partition<GA>(cg::this_thread_block());
+  const int lane = tile.thread_rank();
+  const int row = (int)(((int64_t)blockIdx.x * 256 + threadIdx.x) / GA);
+  long long ip = 0;
+  if (row < n) {
+    const int a0 = arpt[row], a1 = arpt[row + 1];
+    for (int j = a0 + lane; j < a1; j += GA) {
+      const int k = ld_stream(acol + j);
+      ip += brpt[k + 1] - brpt[k];
+    }
+  }
+  ip = cg::reduce(tile, ip, cg::plus<long long>());
+  if (lane == 0 && row < n) {
+    const int ub = (int)(ip < (long long)ncols_b ? ip : (long long)ncols_b);
+    row_nz[row] = ub;
+    if (row_ip) row_ip[row] = ip;
+    if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
+    if (ip) atomicAdd(&s_total, (unsigned long long)ip);
+  }
+  __syncthreads();
+  if (threadIdx.x < kSymBins && hist[threadIdx.x])
+    atomicAdd(&sym_counts[threadIdx.x], hist[threadIdx.x]);
+  if (threadIdx.x == 0 && s_total) atomicAdd(total_ip, s_total);
+}
+
+cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
+                           int64_t *row_ip, int *sym_counts,
+                           unsigned long long *total_ip, cudaStream_t s) {
+  const int n = A.nrows;
+  if (n <= 0) return cudaSuccess;
+  const double avg = (double)A.nnz / (double)n;
+  const int ga = avg > 24.0 ? 32 : avg > 12.0 ? 16 : avg > 6.0 ? 8 : 4;
+  const int grid = (int)(((int64_t)n * ga + 255) / 256);
+  switch (ga) {
+    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
+    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
+    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
+    default: k_rowinfo<4><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
+  }
+  return cudaGetLastError();
+}
+
+// ---- bin permutation ------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+    k_perm(const int *__restrict__ key, int n, int kind, BinOffsets off,
+           int *__restrict__ cursor, int *__restrict__ perm) {
+  __shared__ int hist[16];
+  __shared__ int base[16];
+  if (threadIdx.x < 16) hist[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  int b = -1, r = 0;
+  if (i < n) {
+    const int k = kind == 0 ? key[i] : key[i + 1] - key[i];
+    if (k > 0) {
+      b = kind == 0 ? sym_bin(k) : num_bin(k);
+      r = atomicAdd(&hist[b], 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 16 && hist[threadIdx.x])
+    base[threadIdx.x] = off.v[threadIdx.x] + atomicAdd(&cursor[threadIdx.x], hist[threadIdx.x]);
+  __syncthreads();
+  if (b >= 0) perm[base[b] + r] = i;
+}
+
+cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets,
+                        int *cursor, int *perm, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_perm<<<(n + 1023) / 1024, 1024, 0, s>>>(key, n, kind, offsets, cursor, perm);
+  return cudaGetLastError();
+}
+
+// ---- single-pass exclusive scan with decoupled look-back -----------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr unsigned long long kAggregate = 1ull, kInclusive = 2ull;
+constexpr int kWaitLimit = 1 << 22;  // ~0.3 s of polling before the error word is set
+
+int scan_tiles(int n) { return n <= 0 ? 1 : (n + kScanTile - 1) / kScanTile; }
+
+__device__ __forceinline__ void publish(unsigned long long *st, int t, long long v,
+                                        unsigned long long flag) {
+  *((volatile unsigned long long *)(st + t)) = ((unsigned long long)v << 2) | flag;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan(const int *__restrict__ in, int n, int *__restrict__ out,
+           long long *__restrict__ total, unsigned long long *tile_state,
+           int *tile_ctr, int *__restrict__ num_counts, int *__restrict__ err) {
+  __shared__ int s_tile;
+  __shared__ long long s_warp[kScanThreads / 32];
+  __shared__ long long s_prefix;
+  __shared__ int hist[kNumBins];
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1);
+  if (threadIdx.x < kNumBins) hist[threadIdx.x] = 0;
+  __syncthreads();
+  const int tile = s_tile;
+  const long long base = (long long)tile * kScanTile + (long long)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  if (base + kScanItems <= n) {
+    const int4 *p = reinterpret_cast<const int4 *>(in + base);
+    const int4 x = p[0], y = p[1];
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) v[q] = base + q < n ? in[base + q] : 0;
+  }
+  long long sum = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    sum += v[q];
+    if (v[q] > 0) atomicAdd(&hist[num_bin(v[q])], 1);
+  }
+  // block scan of the per-thread sums
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  long long incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    long long w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    if (lane < kScanThreads / 32) s_warp[lane] = w;  // inclusive warp prefixes
+  }
+  __syncthreads();
+  const long long block_total = s_warp[kScanThreads / 32 - 1];
+  const long long excl = (warp ? s_warp[warp - 1] : 0) + incl - sum;
+  if (threadIdx.x == 0) {
+    long long prefix = 0;
+    if (tile == 0) {
+      publish(tile_state, 0, block_total, kInclusive);
+    } else {
+      publish(tile_state, tile, block_total, kAggregate);
+      for (int p = tile - 1; p >= 0; --p) {
+        unsigned long long st = *((volatile unsigned long long *)(tile_state + p));
+        int spins = 0;
+        while ((st & 3ull) == 0ull) {
+          if (++spins > kWaitLimit) {
+            atomicOr(err, ERR_WAIT);
+            st = kInclusive;  // give up: treat as a zero inclusive prefix
+            break;
+          }
+          __nanosleep(64);
+          st = *((volatile unsigned long long *)(tile_state + p));
+        }
+        prefix += (long long)(st >> 2);
+        if ((st & 3ull) == kInclusive) break;
+      }
+      publish(tile_state, tile, prefix + block_total, kInclusive);
+    }
+    s_prefix = prefix;
+  }
+  __syncthreads();
+  long long run = s_prefix + excl;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    if (base + q < n) out[base + q] = run > 0x7fffffffLL ? 0x7fffffff : (int)run;
+    run += v[q];
+  }
+  if (base < n && base + kScanItems >= n) {  // the thread holding row n-1
+    out[n] = run > 0x7fffffffLL ? 0x7fffffff : (int)run;
+    *total = run;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNumBins && hist[threadIdx.x])
+    atomicAdd(&num_counts[threadIdx.x], hist[threadIdx.x]);
+}
+
+cudaError_t launch_scan(const int *row_nz, int n, int *crpt, long long *total,
+                        unsigned long long *tile_state, int *tile_ctr,
+                        int *num_counts, int *err, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_scan<<<scan_tiles(n), kScanThreads, 0, s>>>(row_nz, n, crpt, total, tile_state,
+                                                tile_ctr, num_counts, err);
+  return cudaGetLastError();
+}
+
+// ---- numeric bins from an existing row pointer ---------------------------------
+__global__ void __launch_bounds__(1024)
+    k_num_hist(const int *__restrict__ crpt, int n, int *__restrict__ num_counts) {
+  __shared__ int hist[kNumBins];
+  if (threadIdx.x < kNumBins) hist[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) {
+    const int k = crpt[i + 1] - crpt[i];
+    if (k > 0) atomicAdd(&hist[num_bin(k)], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < kNumBins && hist[threadIdx.x])
+    atomicAdd(&num_counts[threadIdx.x], hist[threadIdx.x]);
+}
+
+cudaError_t launch_num_hist(const int *crpt, int n, int *num_counts, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_num_hist<<<(n + 1023) / 1024, 1024, 0, s>>>(crpt, n, num_counts);
+  return cudaGetLastError();
+}
+
+}  // namespace nspb

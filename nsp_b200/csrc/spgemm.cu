@@ -1,0 +1,542 @@
+// Host orchestration of the CSR product and the C ABI entry points.
+//
+// Flow of one product C = A·B on one stream (compare nsp_spgemm_kernel_hash,
+// nsp/src/nsp.cu:2448-2488, which creates 11 streams, calls cudaMalloc and
+// cudaFree for its scratch on every call, and synchronises the host 4-6 times):
+//   1. B row-order check (skipped with opts.assume_sorted)
+//   2. intermediate products per row -> symbolic bins          (host sync #1)
+//   3. bin permutation (skipped when one bin holds every row)
+//   4. one persistent kernel per non-empty symbolic bin
+//   5. single-pass scan row_nz -> C.rowptr, numeric-bin histogram (host sync #2)
+//   6. C.col / C.val allocated (unless provided)
+//   7. bin permutation + one persistent kernel per non-empty numeric bin
+// Scratch comes from a library-owned stream-ordered memory pool, so repeated
+// calls do not call cudaMalloc for it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+#include "internal.h"
+#include "spgemm_host.h"
+
+namespace nspb {
+
+thread_local int g_last_cuda = 0;
+
+const DevInfo &dev_info() {
+  static std::mutex mu;
+  static DevInfo infos[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  DevInfo &d = infos[dev];
+  if (d.device < 0) {
+    cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    d.device = dev;
+  }
+  return d;
+}
+
+// Library-owned stream-ordered pool per device; freed blocks stay cached.
+static cudaMemPool_t scratch_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
+int scratch_alloc(void **p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool = scratch_pool();
+  if (!pool) return NSPB_ERR_ALLOC;
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes < 256 ? 256 : bytes, pool, s);
+  if (e != cudaSuccess) {
+    g_last_cuda = (int)e;
+    cudaGetLastError();
+    return NSPB_ERR_ALLOC;
+  }
+  return NSPB_OK;
+}
+
+void scratch_free(void *p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+// Pinned staging for the two small device->host reads of a call.
+HostStage *host_stage() {
+  struct Holder {
+    HostStage *p = nullptr;
+    ~Holder() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  static thread_local Holder h;
+  if (!h.p) {
+    void *q = nullptr;
+    if (cudaMallocHost(&q, sizeof(HostStage)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    h.p = static_cast<HostStage *>(q);
+  }
+  return h.p;
+}
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// ---- a call --------------------------------------------------------------------
+int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
+  nspb_default_opts(&opts);
+  if (o) opts = *o;
+  s = static_cast<cudaStream_t>(opts.stream);
+  if (!a || !b) return NSPB_ERR_INVALID;
+  if (a->nrows < 0 || a->ncols < 0 || b->nrows < 0 || b->ncols < 0) return NSPB_ERR_INVALID;
+  if (a->ncols != b->nrows) return NSPB_ERR_INVALID;
+  if (a->nnz < 0 || b->nnz < 0 || a->nnz > INT32_MAX || b->nnz > INT32_MAX) return NSPB_ERR_INVALID;
+  if ((a->nrows > 0 && !a->rowptr) || (b->nrows > 0 && !b->rowptr)) return NSPB_ERR_INVALID;
+  if ((a->nnz > 0 && (!a->col || !a->val)) || (b->nnz > 0 && (!b->col || !b->val)))
+    return NSPB_ERR_INVALID;
+  const int want = opts.precision == NSPB_PREC_FP32_COMP ? NSPB_F32 : NSPB_F64;
+  if (opts.precision != NSPB_PREC_FP64 && opts.precision != NSPB_PREC_FP32_COMP)
+    return NSPB_ERR_INVALID;
+  if ((a->nnz > 0 && a->val_type != want) || (b->nnz > 0 && b->val_type != want))
+    return NSPB_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return NSPB_ERR_NO_DEVICE;
+  }
+  auto fill = [&](CsrDev &d, const nspb_csr_in *m) {
+    d.nrows = m->nrows;
+    d.ncols = m->ncols;
+    d.nnz = m->nnz;
+    d.rpt = m->rowptr;
+    d.col = m->col;
+    if (m->val_type == NSPB_F32) d.val32 = static_cast<const float *>(m->val);
+    else d.val = static_cast<const double *>(m->val);
+  };
+  fill(A, a);
+  fill(B, b);
+  n = A.nrows;
+  if (opts.timing) {
+    timing = true;
+    for (auto &e : ev) cudaEventCreate(&e);
+  }
+  if (opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32) {
+    lanes = opts.group_lanes;
+  } else {
+    const double avg = B.nrows > 0 ? (double)B.nnz / (double)B.nrows : 0.0;
+    lanes = avg <= 8.0 ? 8 : avg <= 16.0 ? 16 : 32;
+  }
+  return NSPB_OK;
+}
+
+int Call::alloc_scratch() {
+  const size_t nn = (size_t)std::max(n, 1);
+  off_row_nz = 0;
+  off_perm = align256(off_row_nz + (nn + 1) * 4);
+  off_counters = align256(off_perm + nn * 4);
+  off_tiles = align256(off_counters + sizeof(DevCounters));
+  const size_t tiles = (size_t)scan_tiles(n);
+  ws_bytes = align256(off_tiles + tiles * 8);
+  int st = scratch_alloc(reinterpret_cast<void **>(&ws), ws_bytes, s);
+  if (st) return st;
+  row_nz = reinterpret_cast<int *>(ws + off_row_nz);
+  perm = reinterpret_cast<int *>(ws + off_perm);
+  ctr = reinterpret_cast<DevCounters *>(ws + off_counters);
+  tile_state = reinterpret_cast<unsigned long long *>(ws + off_tiles);
+  // counters and scan tile states are contiguous: one memset clears both
+  cudaError_t e = cudaMemsetAsync(ws + off_counters, 0, ws_bytes - off_counters, s);
+  if (e != cudaSuccess) return cuda_fail(e);
+  return NSPB_OK;
+}
+
+Call::~Call() {
+  if (ws) scratch_free(ws, s);
+  for (auto &e : ev)
+    if (e) cudaEventDestroy(e);
+}
+
+int Call::cuda_fail(cudaError_t e) {
+  g_last_cuda = (int)e;
+  cudaGetLastError();
+  return NSPB_ERR_CUDA;
+}
+
+int Call::fetch_counters() {
+  HostStage *hs = host_stage();
+  if (!hs) return NSPB_ERR_ALLOC;
+  cudaError_t e = cudaMemcpyAsync(&hs->c, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(e);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e);
+  h = hs->c;
+  if (h.err) return NSPB_ERR_DEVICE;
+  return NSPB_OK;
+}
+
+static BinOffsets offsets_of(const int *counts, int nb, int *nonempty, int *total) {
+  BinOffsets o;
+  int acc = 0, ne = 0;
+  for (int b = 0; b < 16; ++b) {
+    o.v[b] = acc;
+    if (b < nb) {
+      acc += counts[b];
+      ne += counts[b] > 0;
+    }
+  }
+  *nonempty = ne;
+  *total = acc;
+  return o;
+}
+
+// Steps 1-5: C.rowptr and nnz(C). crpt must hold n+1 ints.
+int Call::symbolic(int *crpt, int64_t *nnz_out) {
+  cudaError_t e;
+  if (n == 0) {
+    e = cudaMemsetAsync(crpt, 0, sizeof(int), s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    *nnz_out = 0;
+    return NSPB_OK;
+  }
+  int st = alloc_scratch();
+  if (st) return st;
+  mark(0);
+  if (!opts.assume_sorted) {
+    if ((e = launch_check_sorted(B, &ctr->flags, s)) != cudaSuccess) return cuda_fail(e);
+    ++launches;
+  }
+  if ((e = launch_rowinfo(A, B, row_nz, nullptr, ctr->sym_counts, &ctr->total_ip, s)) != cudaSuccess)
+    return cuda_fail(e);
+  ++launches;
+  mark(1);
+  if ((st = fetch_counters())) return st;
+  b_sorted = opts.assume_sorted || !(h.flags & B_UNSORTED);
+  intprod = (int64_t)h.total_ip;
+  int nonempty = 0, binned = 0;
+  BinOffsets off = offsets_of(h.sym_counts, kSymBins, &nonempty, &binned);
+  const bool direct = nonempty == 1 && binned == n;
+  mark(2);
+  if (!direct && binned > 0) {
+    if ((e = launch_perm(row_nz, n, 0, off, ctr->cursor_sym, perm, s)) != cudaSuccess)
+      return cuda_fail(e);
+    ++launches;
+  }
+  for (int b = 0; b < kSymBins; ++b) {
+    const int c = h.sym_counts[b];
+    if (c <= 0) continue;
+    e = launch_symbolic_bin(b, lanes, A, B, direct ? nullptr : perm + off.v[b], c, row_nz,
+                            &ctr->err, s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    ++launches;
+  }
+  mark(3);
+  if ((e = launch_scan(row_nz, n, crpt, &ctr->total_nnz, tile_state, &ctr->tile_ctr,
+                       ctr->num_counts, &ctr->err, s)) != cudaSuccess)
+    return cuda_fail(e);
+  ++launches;
+  mark(4);
+  if ((st = fetch_counters())) return st;
+  num_counts_ready = true;
+  if (h.total_nnz > INT32_MAX) return NSPB_ERR_OVERFLOW;
+  *nnz_out = h.total_nnz;
+  return NSPB_OK;
+}
+
+// Step 7 (the numeric-bin histogram must be in h.num_counts).
+int Call::numeric(const int *crpt, int *ccol, double *cval) {
+  cudaError_t e;
+  if (n == 0) return NSPB_OK;
+  int nonempty = 0, binned = 0;
+  BinOffsets off = offsets_of(h.num_counts, kNumBins, &nonempty, &binned);
+  if (binned == 0) return NSPB_OK;
+  const bool direct = nonempty == 1 && binned == n;
+  mark(5);
+  if (!direct) {
+    if ((e = launch_perm(crpt, n, 1, off, ctr->cursor_num, perm, s)) != cudaSuccess)
+      return cuda_fail(e);
+    ++launches;
+  }
+  for (int b = 0; b < kNumBins; ++b) {
+    const int c = h.num_counts[b];
+    if (c <= 0) continue;
+    e = launch_numeric_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval,
+                           direct ? nullptr : perm + off.v[b], c, &ctr->err, s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    ++launches;
+  }
+  mark(6);
+  return NSPB_OK;
+}
+
+// Numeric bins and B order for a two-call numeric step.
+int Call::prepare_numeric(const int *crpt) {
+  if (n == 0) return NSPB_OK;
+  int st = alloc_scratch();
+  if (st) return st;
+  cudaError_t e;
+  if (!opts.assume_sorted && (e = launch_check_sorted(B, &ctr->flags, s)) != cudaSuccess)
+    return cuda_fail(e);
+  if ((e = launch_num_hist(crpt, n, ctr->num_counts, s)) != cudaSuccess) return cuda_fail(e);
+  launches += opts.assume_sorted ? 1 : 2;
+  if ((st = fetch_counters())) return st;
+  b_sorted = opts.assume_sorted || !(h.flags & B_UNSORTED);
+  num_counts_ready = true;
+  return NSPB_OK;
+}
+
+int Call::finish(nspb_stats *stats) {
+  if (opts.check_errors && n > 0) {
+    int st = fetch_counters();
+    if (st) return st;
+  }
+  if (stats) {
+    stats->intprod = intprod;
+    stats->nnz = h.total_nnz;
+    for (int b = 0; b < 16; ++b) {
+      stats->sym_bins[b] = b < kSymBins ? h.sym_counts[b] : 0;
+      stats->num_bins[b] = b < kNumBins ? h.num_counts[b] : 0;
+    }
+    stats->b_sorted = b_sorted ? 1 : 0;
+    stats->launches = launches;
+    stats->ms_rowinfo = stats->ms_symbolic = stats->ms_scan = stats->ms_numeric = 0.f;
+    if (timing && n > 0) {
+      cudaStreamSynchronize(s);
+      auto span = [&](int a, int b) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev[a], ev[b]) != cudaSuccess) {
+          cudaGetLastError();
+          ms = 0.f;
+        }
+        return ms;
+      };
+      stats->ms_rowinfo = span(0, 1);
+      stats->ms_symbolic = span(2, 3);
+      stats->ms_scan = span(3, 4);
+      stats->ms_numeric = span(5, 6);
+    }
+  }
+  return NSPB_OK;
+}
+
+int alloc_out(void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes < 4 ? 4 : bytes);
+  if (e != cudaSuccess) {
+    g_last_cuda = (int)e;
+    cudaGetLastError();
+    return NSPB_ERR_ALLOC;
+  }
+  return NSPB_OK;
+}
+
+}  // namespace nspb
+
+using namespace nspb;
+
+extern "C" {
+
+const char *nspb_version(void) { return "nspb 0.1 (sm_100a)"; }
+
+const char *nspb_strerror(int status) {
+  switch (status) {
+    case NSPB_OK: return "success";
+    case NSPB_ERR_INVALID: return "invalid argument";
+    case NSPB_ERR_OVERFLOW: return "nnz(C) or a row count exceeds int32";
+    case NSPB_ERR_ALLOC: return "allocation failed";
+    case NSPB_ERR_CUDA: return "CUDA runtime error";
+    case NSPB_ERR_DEVICE: return "device error word set (bounded probe or wait exhausted)";
+    case NSPB_ERR_NO_DEVICE: return "no CUDA device";
+    case NSPB_ERR_UNSUPPORTED: return "unsupported";
+    case NSPB_ERR_CAPACITY: return "output capacity too small";
+    default: return "unknown status";
+  }
+}
+
+int nspb_last_cuda_error(void) { return g_last_cuda; }
+
+void nspb_default_opts(nspb_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = NSPB_PREC_FP64;
+  o->comp_tol = 1e-12;
+}
+
+int nspb_free(void *p) {
+  if (!p) return NSPB_OK;
+  cudaError_t e = cudaFree(p);
+  if (e != cudaSuccess) {
+    g_last_cuda = (int)e;
+    cudaGetLastError();
+    return NSPB_ERR_CUDA;
+  }
+  return NSPB_OK;
+}
+
+int nspb_device_sm_count(int *sms) {
+  int ndev = 0;
+  if (!sms) return NSPB_ERR_INVALID;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return NSPB_ERR_NO_DEVICE;
+  }
+  *sms = dev_info().sms;
+  return NSPB_OK;
+}
+
+int nspb_spgemm_symbolic(const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
+                         const nspb_opts *opts, nspb_stats *stats) {
+  if (!C) return NSPB_ERR_INVALID;
+  Call call;
+  int st = call.init(A, B, opts);
+  if (st) return st;
+  bool own_rpt = false;
+  if (!C->rowptr) {
+    if ((st = alloc_out(reinterpret_cast<void **>(&C->rowptr), ((size_t)call.n + 1) * 4))) return st;
+    own_rpt = true;
+  }
+  int64_t nnz = 0;
+  st = call.symbolic(C->rowptr, &nnz);
+  if (!st) st = call.finish(stats);
+  if (st) {
+    if (own_rpt) {
+      cudaStreamSynchronize(call.s);
+      cudaFree(C->rowptr);
+      C->rowptr = nullptr;
+    }
+    return st;
+  }
+  C->nrows = A->nrows;
+  C->ncols = B->ncols;
+  C->nnz = nnz;
+  return NSPB_OK;
+}
+
+int nspb_spgemm_numeric(const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
+                        const nspb_opts *opts, nspb_stats *stats) {
+  if (!C || !C->rowptr) return NSPB_ERR_INVALID;
+  Call call;
+  int st = call.init(A, B, opts);
+  if (st) return st;
+  if (C->nnz < 0 || C->nnz > INT32_MAX) return NSPB_ERR_INVALID;
+  if ((C->col || C->val) && (!C->col || !C->val)) return NSPB_ERR_INVALID;
+  if (C->col && C->capacity < C->nnz) return NSPB_ERR_CAPACITY;
+  if ((st = call.prepare_numeric(C->rowptr))) return st;
+  call.h.total_nnz = C->nnz;
+  bool own = false;
+  if (!C->col) {
+    if ((st = alloc_out(reinterpret_cast<void **>(&C->col), (size_t)C->nnz * 4))) return st;
+    if ((st = alloc_out(reinterpret_cast<void **>(&C->val), (size_t)C->nnz * 8))) {
+      cudaFree(C->col);
+      C->col = nullptr;
+      return st;
+    }
+    own = true;
+    C->capacity = C->nnz;
+  }
+  st = run_numeric_mode(call, C);
+  if (!st) st = call.finish(stats);
+  if (st && own) {
+    cudaStreamSynchronize(call.s);
+    cudaFree(C->col);
+    cudaFree(C->val);
+    C->col = nullptr;
+    C->val = nullptr;
+  }
+  return st;
+}
+
+int nspb_spgemm(const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
+                const nspb_opts *opts, nspb_stats *stats) {
+  if (!C) return NSPB_ERR_INVALID;
+  if ((C->col || C->val) && (!C->col || !C->val)) return NSPB_ERR_INVALID;
+  Call call;
+  int st = call.init(A, B, opts);
+  if (st) return st;
+  bool own_rpt = false, own_cv = false;
+  if (!C->rowptr) {
+    if ((st = alloc_out(reinterpret_cast<void **>(&C->rowptr), ((size_t)call.n + 1) * 4))) return st;
+    own_rpt = true;
+  }
+  int64_t nnz = 0;
+  st = call.symbolic(C->rowptr, &nnz);
+  if (!st) {
+    if (!C->col) {
+      st = alloc_out(reinterpret_cast<void **>(&C->col), (size_t)nnz * 4);
+      if (!st) {
+        st = alloc_out(reinterpret_cast<void **>(&C->val), (size_t)nnz * 8);
+        if (st) {
+          cudaFree(C->col);
+          C->col = nullptr;
+        }
+      }
+      own_cv = !st;
+      if (!st) C->capacity = nnz;
+    } else if (C->capacity < nnz) {
+      st = NSPB_ERR_CAPACITY;
+    }
+  }
+  if (!st) st = run_numeric_mode(call, C);
+  if (!st) st = call.finish(stats);
+  if (st) {
+    cudaStreamSynchronize(call.s);
+    if (own_cv) {
+      cudaFree(C->col);
+      cudaFree(C->val);
+      C->col = nullptr;
+      C->val = nullptr;
+    }
+    if (own_rpt) {
+      cudaFree(C->rowptr);
+      C->rowptr = nullptr;
+    }
+    return st;
+  }
+  C->nrows = A->nrows;
+  C->ncols = B->ncols;
+  C->nnz = nnz;
+  return NSPB_OK;
+}
+
+int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip, int64_t *total,
+                 void *stream) {
+  nspb_opts o;
+  nspb_default_opts(&o);
+  o.stream = stream;
+  o.assume_sorted = 1;
+  // values are not read: accept either value type
+  o.precision = (A && A->val_type == NSPB_F32) ? NSPB_PREC_FP32_COMP : NSPB_PREC_FP64;
+  Call call;
+  int st = call.init(A, B, &o);
+  if (st) return st;
+  if (call.n == 0) {
+    if (total) *total = 0;
+    return NSPB_OK;
+  }
+  if ((st = call.alloc_scratch())) return st;
+  cudaError_t e = launch_rowinfo(call.A, call.B, call.row_nz, d_row_ip, call.ctr->sym_counts,
+                                 &call.ctr->total_ip, call.s);
+  if (e != cudaSuccess) return call.cuda_fail(e);
+  if ((st = call.fetch_counters())) return st;
+  if (total) *total = (int64_t)call.h.total_ip;
+  return NSPB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+// Host-side state of one product call (shared by the one-call, two-call,
+// FP32-compensated, batched and row-blocked entry points).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace nspb {
+
+extern thread_local int g_last_cuda;
+
+// Device counters of a call, zeroed at the start; read back in one copy.
+struct DevCounters {
+  int sym_counts[16];
+  int num_counts[16];
+  int cursor_sym[16];
+  int cursor_num[16];
+  int flags;
+  int err;
+  int tile_ctr;
+  int redo_count;
+  unsigned long long total_ip;
+  long long total_nnz;
+  float max_row_err;
+  int pad[3];
+};
+
+struct HostStage {
+  DevCounters c;
+};
+
+HostStage *host_stage();
+int scratch_alloc(void **p, size_t bytes, cudaStream_t s);
+void scratch_free(void *p, cudaStream_t s);
+int alloc_out(void **p, size_t bytes);
+
+struct Call {
+  nspb_opts opts{};
+  cudaStream_t s = nullptr;
+  CsrDev A, B;
+  int n = 0;
+  int lanes = 32;
+  // scratch (one stream-ordered block)
+  char *ws = nullptr;
+  size_t ws_bytes = 0;
+  size_t off_row_nz = 0, off_perm = 0, off_counters = 0, off_tiles = 0;
+  int *row_nz = nullptr;
+  int *perm = nullptr;
+  DevCounters *ctr = nullptr;
+  unsigned long long *tile_state = nullptr;
+  // host copies
+  DevCounters h{};
+  bool b_sorted = true;
+  bool num_counts_ready = false;
+  int64_t intprod = 0;
+  int launches = 0;
+  // opts.timing: events around rowinfo, symbolic, scan, numeric
+  cudaEvent_t ev[8] = {};
+  bool timing = false;
+  void mark(int i) {
+    if (timing && ev[i]) cudaEventRecord(ev[i], s);
+  }
+
+  int init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o);
+  int alloc_scratch();
+  int cuda_fail(cudaError_t e);
+  int fetch_counters();
+  int symbolic(int *crpt, int64_t *nnz_out);
+  int prepare_numeric(const int *crpt);
+  int numeric(const int *crpt, int *ccol, double *cval);
+  int finish(nspb_stats *stats);
+  ~Call();
+};
+
+// Numeric step in the call's precision mode (fp64 or fp32-compensated).
+int run_numeric_mode(Call &call, nspb_csr_out *C);
+
+}  // namespace nspb

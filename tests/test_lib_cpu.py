@@ -1,0 +1,70 @@
+"""The C-ABI library loads and exports every symbol its headers declare
+(no compute calls: these run without a GPU)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+import nsp_b200 as nb
+from nsp_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_c_functions():
+    names = set()
+    for h in ("nspb.h", "nspb_compat.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b(nspb_\w+)\s*\(", src))
+    return sorted(names)
+
+
+def test_headers_declare_entry_points():
+    names = declared_c_functions()
+    assert "nspb_spgemm" in names and "nspb_nsp_spgemm_kernel_hash" in names
+    assert len(names) >= 20
+
+
+@pytest.mark.parametrize("name", declared_c_functions())
+def test_c_symbol_exported(name):
+    assert hasattr(_lib.lib, name), f"{name} missing from libnspb.so"
+
+
+def test_cpp_shims_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    for sym in ("_Z22nsp_spgemm_kernel_hashP5sfCSRS0_S0_",
+                "nsparseMGPU_version0", "nsparseMGPU_version1"):
+        assert sym in out, sym
+
+
+def test_strerror_and_defaults():
+    assert nb.lib.nspb_strerror(0) == b"success"
+    assert b"int32" in nb.lib.nspb_strerror(_lib.ERR_OVERFLOW)
+    o = _lib.Opts()
+    nb.lib.nspb_default_opts(ctypes.byref(o))
+    assert o.precision == _lib.PREC_FP64 and o.comp_tol == 1e-12
+
+
+def test_generator_thread_independent():
+    code = ("import nsp_b200 as nb, hashlib; P = nb.gen.powerlaw(20000, max_deg=2000, seed=3);"
+            "print(hashlib.sha1(P.col.tobytes() + P.val.tobytes()).hexdigest())")
+    outs = set()
+    for th in ("1", "4"):
+        env = dict(os.environ, OMP_NUM_THREADS=th)
+        outs.add(subprocess.run(["python", "-c", code], cwd=ROOT, env=env, capture_output=True,
+                                text=True, check=True).stdout.strip())
+    assert len(outs) == 1
+
+
+def test_no_device_reports_status():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    a = _lib.CsrIn()
+    c = _lib.CsrOut()
+    st = nb.lib.nspb_spgemm(ctypes.byref(a), ctypes.byref(a), ctypes.byref(c), None, None)
+    assert st == _lib.ERR_NO_DEVICE
