@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--impl", default="nspb", choices=["nspb", "reference"])
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--grid", type=int, default=128,
+                   help="stencil edge L (default 128; smaller grids for profiler captures)")
     return p.parse_args()
 
 
@@ -209,7 +211,12 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global L, METRIC, WORKLOAD
     args = parse()
+    if args.grid != L:
+        L = args.grid
+        METRIC = f"SpGEMM GFLOP/s, C=A*A, 27-point stencil {L}^3, fp64"
+        WORKLOAD = f"stencil27_{L}^3_AxA_fp64"
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
@@ -390,7 +397,8 @@ def main():
             "config": {"workload": WORKLOAD, "grid": [L, L, L * world], "n_rows_per_gpu": dA.nrows,
                        "nnz_A_per_gpu": dA.nnz, "intprod_per_gpu": intprod,
                        "nnz_C_per_gpu": nnz_c,
-                       "l2": "inputs (669 MB) and C (3.06 GB) exceed the 126 MB L2; no flush",
+                       "l2": f"inputs ({12 * dA.nnz / 1e6:.0f} MB) and C ({12 * nnz_c / 1e9:.2f} GB) "
+                             "exceed the 126 MB L2; no flush",
                        "parallelism": "row z-slabs per GPU, halo planes generated locally, "
                                       "no collective"},
             "effective_gbs": gbs,

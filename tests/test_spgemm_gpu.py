@@ -139,7 +139,8 @@ def test_two_call_matches_one_call(cuda):
     rp, nnz = nb.spgemm_symbolic(dA, dB)
     two = nb.spgemm_numeric(dA, dB, rp, nnz).to_host()
     assert_same_structure(two.rowptr, two.col, one.rowptr, one.col)
-    assert_bitwise(two.val, one.val)
+    # rows on the block path add with shared-memory atomics: order may vary
+    assert_close(two.val, one.val, oracle.absbound(A, B, one.rowptr, one.col))
 
 
 def test_caller_provided_output_and_capacity(cuda):
