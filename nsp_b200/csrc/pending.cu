@@ -11,9 +11,6 @@ int run_numeric_mode(Call &call, nspb_csr_out *C) {
 extern "C" {
 int nspb_spgemm_batched(int, const nspb_csr_in *, const nspb_csr_in *, nspb_csr_out *,
                         const nspb_opts *, nspb_stats *) { return NSPB_ERR_UNSUPPORTED; }
-int nspb_getmct(const int32_t *, int64_t, int32_t, int32_t, int32_t *, int64_t *, void *) { return NSPB_ERR_UNSUPPORTED; }
-int nspb_compactcol(const int32_t *, int64_t, int32_t, int32_t, int32_t *, int64_t *, void *) { return NSPB_ERR_UNSUPPORTED; }
-int nspb_shrink_col(const int32_t *, int64_t, const int32_t *, int64_t, int32_t *, void *) { return NSPB_ERR_UNSUPPORTED; }
 int nspb_spgemm_rowblocked(const nspb_csr_in *, const nspb_csr_in *, int64_t, int32_t *, int32_t *,
                            double *, int64_t, int64_t *, int32_t *, const nspb_opts *) { return NSPB_ERR_UNSUPPORTED; }
 }

@@ -42,7 +42,7 @@ def main():
     lib = C.CDLL(oracle.REF_SO)
     lib.ref_nsp_time_device.restype = C.c_float
     lib.ref_nsp_time_device.argtypes = [C.c_int] * 3 + [C.c_void_p] * 3 + [C.c_int] + \
-        [C.c_void_p] * 3 + [C.c_int] * 4 + [C.POINTER(C.c_int)]
+        [C.c_void_p] * 3 + [C.c_int] * 3 + [C.POINTER(C.c_int)]
     nnz = C.c_int(0)
     p = (dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr())
     ref_ms = lib.ref_nsp_time_device(A.nrows, A.ncols, A.ncols, *p, A.nnz, *p, A.nnz,
