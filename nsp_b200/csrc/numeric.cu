@@ -28,12 +28,11 @@ template <int G, int LOG2T>
 struct NumGroupCfg {
   static constexpr int T = 1 << LOG2T;  // hash slots
   static constexpr int H = T / 2;       // max entries of a row in this bin
-  // sort buckets: ~4 per entry for small rows, so runs of clustered columns
-  // rarely share one; 2 per entry above 128 entries
-  static constexpr int NB = H <= 128 ? 4 * H : 2 * H;
-  static constexpr int NBP = NB + NB / 32;  // padded: see cpad()
-  static constexpr int BYTES = T * 12 + H * 12 + NBP * 4;
-  static constexpr int kBySmem = (64 * 1024) / BYTES > 0 ? (64 * 1024) / BYTES : 1;
+  static constexpr int NB = T / 2;      // sort buckets
+  // per-group stride, rounded to 16 bytes so every group's fp64 arrays stay
+  // 8-byte aligned
+  static constexpr int BYTES = (T * 12 + H * 12 + NB * 4 + 15) & ~15;
+  static constexpr int kBySmem = (56 * 1024) / BYTES > 0 ? (56 * 1024) / BYTES : 1;
   static constexpr int GPC = kBySmem < 256 / G ? kBySmem : 256 / G;
   static constexpr int THREADS = GPC * G;
   static constexpr int SMEM = GPC * BYTES;
@@ -71,7 +70,6 @@ __global__ void __launch_bounds__(256)
     const int a0 = arpt[row], a1 = arpt[row + 1];
     int mn = 0x7fffffff, mx = -1;
     for (int ab = a0; ab < a1; ab += G) {
-      // lanes fetch up to G A entries and their B row bounds at once
       int bs = 0, be = 0;
       double av = 0.0;
       if (ab + lane < a1) {
@@ -81,49 +79,20 @@ __global__ void __launch_bounds__(256)
         be = __ldg(brpt + k + 1);
       }
       const int na = min(G, a1 - ab);
-      // A step covers G consecutive entries of one B row. The gathers of the
-      // next step are issued before the current step is inserted.
-      int t = 0, base = 0, end = 0;
-      for (; t < na; ++t) {
-        base = tile.shfl(bs, t);
-        end = tile.shfl(be, t);
-        if (base < end) break;
-      }
-      double a = tile.shfl(av, t < na ? t : 0);
-      int key = -1;
-      double bv = 0.0;
-      if (t < na && base + lane < end) {
-        key = __ldg(bcol + base + lane);
-        bv = __ldg(bval + base + lane);
-      }
-      while (t < na) {
-        int nt = t, nbase = base + G, nend = end;
-        if (nbase >= nend) {
-          for (++nt; nt < na; ++nt) {
-            nbase = tile.shfl(bs, nt);
-            nend = tile.shfl(be, nt);
-            if (nbase < nend) break;
+      for (int t = 0; t < na; ++t) {
+        const int s0 = tile.shfl(bs, t), s1 = tile.shfl(be, t);
+        const double a = tile.shfl(av, t);
+        for (int base = s0; base < s1; base += G) {
+          const int e = base + lane;
+          if (e < s1) {
+            const int key = __ldg(bcol + e);
+            const double p = __dmul_rn(a, __ldg(bval + e));
+            num_insert<LOG2T, OWNED>(keys, vals, key, p, err);
+            mn = min(mn, key);
+            mx = max(mx, key);
           }
+          if (OWNED) tile.sync();  // next step may hit the same slot
         }
-        const double na_val = tile.shfl(av, nt < na ? nt : 0);
-        int nkey = -1;
-        double nbv = 0.0;
-        if (nt < na && nbase + lane < nend) {
-          nkey = __ldg(bcol + nbase + lane);
-          nbv = __ldg(bval + nbase + lane);
-        }
-        if (key >= 0) {
-          num_insert<LOG2T, OWNED>(keys, vals, key, __dmul_rn(a, bv), err);
-          mn = min(mn, key);
-          mx = max(mx, key);
-        }
-        if (OWNED) tile.sync();  // the next step may hit the same slot
-        t = nt;
-        base = nbase;
-        end = nend;
-        a = na_val;
-        key = nkey;
-        bv = nbv;
       }
     }
     tile.sync();
@@ -132,29 +101,29 @@ __global__ void __launch_bounds__(256)
     mn = cg::reduce(tile, mn, cg::less<int>());
     mx = cg::reduce(tile, mx, cg::greater<int>());
     // -- bucket sort: histogram, scan, scatter, rank within bucket
-    for (int b = lane; b < C::NBP; b += G) cnt[b] = 0;
+    for (int b = lane; b < C::NB; b += G) cnt[b] = 0;
     tile.sync();
     const float scale = n > 0 ? (float)C::NB / (float)((long long)mx - mn + 1) : 0.f;
     for (int s = lane; s < C::T; s += G) {
       const int key = keys[s];
-      if (key >= 0) atomicAdd(&cnt[cpad(bucket_of(key, mn, scale, C::NB))], 1);
+      if (key >= 0) atomicAdd(&cnt[bucket_of(key, mn, scale, C::NB)], 1);
     }
     tile.sync();
-    // exclusive scan of the bucket counts: each lane owns PER consecutive ones
+    int local[C::PER];
     int sum = 0;
+#pragma unroll
     for (int q = 0; q < C::PER; ++q) {
       const int idx = lane * C::PER + q;
-      if (idx < C::NB) sum += cnt[cpad(idx)];
+      local[q] = idx < C::NB ? cnt[idx] : 0;
+      sum += local[q];
     }
     int ex = cg::exclusive_scan(tile, sum, cg::plus<int>());
     const int tot = tile.shfl(ex + sum, G - 1);
+#pragma unroll
     for (int q = 0; q < C::PER; ++q) {
       const int idx = lane * C::PER + q;
-      if (idx < C::NB) {
-        const int v = cnt[cpad(idx)];
-        cnt[cpad(idx)] = ex;
-        ex += v;
-      }
+      if (idx < C::NB) cnt[idx] = ex;
+      ex += local[q];
     }
     tile.sync();
     if (tot != n || n > C::H) {  // symbolic/numeric disagreement: skip the row
@@ -165,7 +134,7 @@ __global__ void __launch_bounds__(256)
     for (int s = lane; s < C::T; s += G) {
       const int key = keys[s];
       if (key >= 0) {
-        const int pos = atomicAdd(&cnt[cpad(bucket_of(key, mn, scale, C::NB))], 1);
+        const int pos = atomicAdd(&cnt[bucket_of(key, mn, scale, C::NB)], 1);
         bkeys[pos] = key;
         bvals[pos] = vals[s];
       }
@@ -174,7 +143,7 @@ __global__ void __launch_bounds__(256)
     for (int q = lane; q < n; q += G) {
       const int key = bkeys[q];
       const int b = bucket_of(key, mn, scale, C::NB);
-      const int st = b ? cnt[cpad(b - 1)] : 0, en = cnt[cpad(b)];
+      const int st = b ? cnt[b - 1] : 0, en = cnt[b];
       int rank = st;
       for (int u = st; u < en; ++u) rank += bkeys[u] < key;
       keys[rank] = key;
@@ -229,7 +198,6 @@ __global__ void __launch_bounds__(kNumBlockThreads)
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
                 int *__restrict__ err) {
   constexpr int T = 1 << LOG2T, H = T / 2, NB = T / 2;
-  constexpr int NBP = NB + NB / 32;
   constexpr int PER = NB / kNumBlockThreads;
   extern __shared__ __align__(16) unsigned char smem_num[];
   double *vals = reinterpret_cast<double *>(smem_num);
@@ -247,7 +215,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
       keys[s] = kEmpty;
       vals[s] = 0.0;
     }
-    for (int b = threadIdx.x; b < NBP; b += kNumBlockThreads) cnt[b] = 0;
+    for (int b = threadIdx.x; b < NB; b += kNumBlockThreads) cnt[b] = 0;
     if (threadIdx.x == 0) {
       s_mn = 0x7fffffff;
       s_mx = -1;
@@ -283,21 +251,21 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     const float scale = n > 0 ? (float)NB / (float)((long long)mx - mn + 1) : 0.f;
     for (int s = threadIdx.x; s < T; s += kNumBlockThreads) {
       const int key = keys[s];
-      if (key >= 0) atomicAdd(&cnt[cpad(bucket_of(key, mn, scale, NB))], 1);
+      if (key >= 0) atomicAdd(&cnt[bucket_of(key, mn, scale, NB)], 1);
     }
     __syncthreads();
     int local[PER];
     int sum = 0;
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
-      local[q] = cnt[cpad(threadIdx.x * PER + q)];
+      local[q] = cnt[threadIdx.x * PER + q];
       sum += local[q];
     }
     int tot;
     int ex = block_exclusive_scan(sum, red, &tot);
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
-      cnt[cpad(threadIdx.x * PER + q)] = ex;
+      cnt[threadIdx.x * PER + q] = ex;
       ex += local[q];
     }
     __syncthreads();
@@ -309,7 +277,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     for (int s = threadIdx.x; s < T; s += kNumBlockThreads) {
       const int key = keys[s];
       if (key >= 0) {
-        const int pos = atomicAdd(&cnt[cpad(bucket_of(key, mn, scale, NB))], 1);
+        const int pos = atomicAdd(&cnt[bucket_of(key, mn, scale, NB)], 1);
         bkeys[pos] = key;
         bvals[pos] = vals[s];
       }
@@ -318,7 +286,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     for (int q = threadIdx.x; q < n; q += kNumBlockThreads) {
       const int key = bkeys[q];
       const int b = bucket_of(key, mn, scale, NB);
-      const int st = b ? cnt[cpad(b - 1)] : 0, en = cnt[cpad(b)];
+      const int st = b ? cnt[b - 1] : 0, en = cnt[b];
       int rank = st;
       for (int u = st; u < en; ++u) rank += bkeys[u] < key;
       keys[rank] = key;
@@ -484,7 +452,7 @@ static cudaError_t run_num_block(const CsrDev &A, const CsrDev &B, const int *cr
                                  double *cval, const int *rows, int count, int *err,
                                  cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
-  const int smem = T * 12 + (T / 2) * 12 + ((T / 2) + (T / 64)) * 4;
+  const int smem = T * 12 + (T / 2) * 12 + (T / 2) * 4;
   const void *f = (const void *)k_num_block<LOG2T>;
   const int grid = persistent_grid(f, kNumBlockThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;

@@ -55,30 +55,10 @@ __global__ void __launch_bounds__(256)
         be = __ldg(brpt + k + 1);
       }
       const int cnt = min(G, a1 - ab);
-      // steps of G consecutive entries of one B row; the next step's keys
-      // are loaded before the current ones are inserted
-      int t = 0, base = 0, end = 0;
-      for (; t < cnt; ++t) {
-        base = tile.shfl(bs, t);
-        end = tile.shfl(be, t);
-        if (base < end) break;
-      }
-      int key = (t < cnt && base + lane < end) ? __ldg(bcol + base + lane) : -1;
-      while (t < cnt) {
-        int nt = t, nbase = base + G, nend = end;
-        if (nbase >= nend) {
-          for (++nt; nt < cnt; ++nt) {
-            nbase = tile.shfl(bs, nt);
-            nend = tile.shfl(be, nt);
-            if (nbase < nend) break;
-          }
-        }
-        const int nkey = (nt < cnt && nbase + lane < nend) ? __ldg(bcol + nbase + lane) : -1;
-        if (key >= 0) nz += sym_insert<LOG2T>(table, key, err);
-        t = nt;
-        base = nbase;
-        end = nend;
-        key = nkey;
+      for (int t = 0; t < cnt; ++t) {
+        const int s0 = tile.shfl(bs, t), s1 = tile.shfl(be, t);
+        for (int e = s0 + lane; e < s1; e += G)
+          nz += sym_insert<LOG2T>(table, __ldg(bcol + e), err);
       }
     }
     nz = cg::reduce(tile, nz, cg::plus<int>());
