@@ -148,6 +148,22 @@ int nspb_spgemm_numeric(const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
                         nspb_stats *stats);
 
+/* No counterpart in the reference. The one-call fp64 product for callers that
+ * may not allocate memory during the call (a framework that owns all device
+ * memory and forbids allocations inside the calls it dispatches, a loop with
+ * memory reserved up front, a process near the HBM limit). C->rowptr, C->col
+ * and C->val must be supplied, with C->capacity entries in col/val
+ * (NSPB_ERR_CAPACITY with C->nnz = the size needed when too small). Scratch
+ * comes from a fixed 32 MiB device array reserved when the library loads, so
+ * A may have at most about 4.19 million rows (4,000,000 always fit); larger
+ * inputs get NSPB_ERR_CAPACITY before any GPU work. Calls share that array:
+ * calls whose GPU work overlaps race, so serialise them. The first call on
+ * each device looks up the array's device address; make it before any stream
+ * capture begins.                                                            */
+int nspb_spgemm_noalloc(const nspb_csr_in *A, const nspb_csr_in *B,
+                        nspb_csr_out *C, const nspb_opts *opts,
+                        nspb_stats *stats);
+
 /* Per-row intermediate-product counts (device out, int64[nrows]) and their
  * total (host out).                                                          */
 int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip,

@@ -157,8 +157,14 @@ int Call::alloc_scratch() {
   off_tiles = align256(off_counters + sizeof(DevCounters));
   const size_t tiles = (size_t)scan_tiles(n);
   ws_bytes = align256(off_tiles + tiles * 8);
-  int st = scratch_alloc(reinterpret_cast<void **>(&ws), ws_bytes, s);
-  if (st) return st;
+  if (ext_ws) {
+    if (ws_bytes > ext_bytes) return NSPB_ERR_CAPACITY;
+    ws = ext_ws;
+    ws_external = true;
+  } else {
+    int st = scratch_alloc(reinterpret_cast<void **>(&ws), ws_bytes, s);
+    if (st) return st;
+  }
   row_nz = reinterpret_cast<int *>(ws + off_row_nz);
   perm = reinterpret_cast<int *>(ws + off_perm);
   ctr = reinterpret_cast<DevCounters *>(ws + off_counters);
@@ -170,7 +176,7 @@ int Call::alloc_scratch() {
 }
 
 Call::~Call() {
-  if (ws) scratch_free(ws, s);
+  if (ws && !ws_external) scratch_free(ws, s);
   for (auto &e : ev)
     if (e) cudaEventDestroy(e);
 }
@@ -182,7 +188,7 @@ int Call::cuda_fail(cudaError_t e) {
 }
 
 int Call::fetch_counters() {
-  HostStage *hs = host_stage();
+  HostStage *hs = stage ? stage : host_stage();
   if (!hs) return NSPB_ERR_ALLOC;
   cudaError_t e = cudaMemcpyAsync(&hs->c, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e);

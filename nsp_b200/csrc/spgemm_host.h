@@ -55,6 +55,12 @@ struct Call {
   bool num_counts_ready = false;
   int64_t intprod = 0;
   int launches = 0;
+  // Caller-supplied scratch and host staging (set by nspb_spgemm_noalloc);
+  // when null the pool and the pinned per-thread stage are used.
+  char *ext_ws = nullptr;
+  size_t ext_bytes = 0;
+  bool ws_external = false;
+  HostStage *stage = nullptr;
   // opts.timing: events around rowinfo, symbolic, scan, numeric
   cudaEvent_t ev[8] = {};
   bool timing = false;
