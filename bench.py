@@ -52,7 +52,128 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--grid", type=int, default=128,
                    help="stencil edge L (default 128; smaller grids for profiler captures)")
+    p.add_argument("--workload", default="stencil27",
+                   choices=["stencil27", "amg_batch", "fp32c"],
+                   help="stencil27: the headline line; amg_batch: batched vs one call per "
+                        "product; fp32c: compensated fp32 vs fp64 on the 27-point stencil")
+    p.add_argument("--batch-count", type=int, default=256)
+    p.add_argument("--batch-nmax", type=int, default=100_000)
     return p.parse_args()
+
+
+def _timed(fn, steps, warmup):
+    """Mean ms of fn() over `steps` after `warmup` calls, CUDA events on the
+    current stream with a synchronize on both sides."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_amg_batch(args):
+    """Batched products (one block-diagonal pipeline) against one nspb_spgemm
+    call per product, on the 6 Galerkin products of the SA-AMG hierarchy of
+    the 27-point stencil on 96^3 plus `batch-count` random products."""
+    import torch
+    import nsp_b200 as nb
+    from nsp_b200 import amg
+    t0 = time.time()
+    pairs = amg.amg_batch(L=96, levels=4, seed=SEED)
+    n_amg = len(pairs)
+    pairs += amg.random_batch(args.batch_count, 1000, args.batch_nmax, 4, 32, seed=SEED)
+    setup_s = time.time() - t0
+    dA = [a.to_device() for a, _ in pairs]
+    dB = [b.to_device() for _, b in pairs]
+    ip = sum(nb.intprod(a, b)[1] for a, b in zip(dA, dB))
+    ip_amg = sum(nb.intprod(a, b)[1] for a, b in zip(dA[:n_amg], dB[:n_amg]))
+    keep = []
+
+    def batched():
+        keep.clear()
+        keep.append(nb.spgemm_batched(dA, dB))
+
+    def single():
+        keep.clear()
+        keep.extend(nb.spgemm(a, b) for a, b in zip(dA, dB))
+
+    def batched_amg():
+        keep.clear()
+        keep.append(nb.spgemm_batched(dA[:n_amg], dB[:n_amg]))
+
+    def single_amg():
+        keep.clear()
+        keep.extend(nb.spgemm(a, b) for a, b in zip(dA[:n_amg], dB[:n_amg]))
+
+    w = max(args.warmup, 1)
+    ms_b = _timed(batched, args.steps, w)
+    ms_s = _timed(single, args.steps, w)
+    ms_ba = _timed(batched_amg, args.steps, w)
+    ms_sa = _timed(single_amg, args.steps, w)
+    keep.clear()
+    print(json.dumps({
+        "metric": "batched SpGEMM GFLOP/s (AMG 96^3 Galerkin products + random products)",
+        "value": 2 * ip / ms_b / 1e6, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": w, "ms_per_step": ms_b, "higher_is_better": True, "dtype": "f64",
+        "data": f"synthetic (seed {SEED})",
+        "config": {"workload": "amg96_galerkin_x6_plus_random", "products": len(pairs),
+                   "random_products": args.batch_count, "random_n": [1000, args.batch_nmax],
+                   "intprod": ip, "setup_s": setup_s},
+        "one_call_per_product": {"value": 2 * ip / ms_s / 1e6, "ms_per_step": ms_s},
+        "speedup_vs_one_call_per_product": ms_s / ms_b,
+        "amg_only": {"products": n_amg, "intprod": ip_amg,
+                     "batched_gflops": 2 * ip_amg / ms_ba / 1e6, "batched_ms": ms_ba,
+                     "one_call_gflops": 2 * ip_amg / ms_sa / 1e6, "one_call_ms": ms_sa}}),
+        flush=True)
+
+
+def run_fp32c(args):
+    """FP32 compensated against fp64 on the 27-point stencil (fp32-representable
+    values): time per product and the error of the fp32 path against the fp64
+    path, scaled by sum_k |a_ik b_kj| = (|A| |B|)_ij computed with the same
+    product on |A|."""
+    import torch
+    import nsp_b200 as nb
+    from nsp_b200.csr import HostCSR
+    Lc = args.grid if args.grid != 128 else 160
+    A = nb.gen.stencil(Lc, npts=27, seed=SEED, fp32=True)
+    d64 = A.to_device()
+    d32 = HostCSR(A.nrows, A.ncols, A.rowptr, A.col, A.val.astype(np.float32)).to_device()
+    ip = nb.intprod(d64, d64)[1]
+    w = max(args.warmup, 1)
+    out64, out32 = [], []
+    ms64 = _timed(lambda: (out64.clear(), out64.append(nb.spgemm(d64, d64))), args.steps, w)
+    st = {}
+
+    def f32():
+        out32.clear()
+        c, s_ = nb.spgemm(d32, d32, precision="fp32c", return_stats=True)
+        out32.append(c)
+        st.update(s_)
+
+    ms32 = _timed(f32, args.steps, w)
+    dabs = nb.DeviceCSR(d64.nrows, d64.ncols, d64.rowptr, d64.col, d64.val.abs())
+    cabs = nb.spgemm(dabs, dabs)
+    c64, c32 = out64[0], out32[0]
+    assert torch.equal(c64.rowptr, c32.rowptr) and torch.equal(c64.col, c32.col)
+    err = ((c32.val - c64.val).abs() / cabs.val.clamp_min(1e-300)).max().item()
+    print(json.dumps({
+        "metric": f"SpGEMM GFLOP/s, C=A*A, 27-point stencil {Lc}^3, fp32 compensated vs fp64",
+        "value": 2 * ip / ms32 / 1e6, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": w, "ms_per_step": ms32, "higher_is_better": True, "dtype": "f32 (compensated)",
+        "data": f"synthetic (seeded 27-point stencil, fp32 values, seed {SEED})",
+        "config": {"workload": f"stencil27_{Lc}^3_AxA", "intprod": ip, "nnz_C": c64.nnz},
+        "fp64": {"value": 2 * ip / ms64 / 1e6, "ms_per_step": ms64},
+        "speedup_vs_fp64": ms64 / ms32,
+        "max_err_vs_fp64_scaled_by_sum_abs": err,
+        "rows_in_fp64": st.get("rows_redone"), "a_priori_bound": st.get("max_row_err")}),
+        flush=True)
 
 
 def dist_env():
@@ -220,6 +341,10 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "amg_batch":
+        return run_amg_batch(args)
+    if args.workload == "fp32c":
+        return run_fp32c(args)
 
     import ctypes as C
     import torch

@@ -101,8 +101,9 @@ typedef struct {
   int32_t group_lanes;   /* 0 = auto; else 8, 16 or 32 lanes per row group    */
   int32_t timing;        /* 1: record CUDA events around each phase (stats)  */
   int32_t _pad;
-  double comp_tol;       /* FP32_COMP: relative error bound per row before the
-                            row is redone in fp64 (default 1e-12 when 0)      */
+  double comp_tol;       /* FP32_COMP: bound on |c - c*| / sum|a*b| per entry;
+                            rows whose a-priori Dot2 bound exceeds it are
+                            accumulated in fp64 (default 1e-10)              */
   void *stream;          /* cudaStream_t                                     */
 } nspb_opts;
 
@@ -112,9 +113,10 @@ typedef struct {
   int64_t nnz;           /* nnz(C)                                           */
   int32_t sym_bins[16];  /* rows per symbolic bin                            */
   int32_t num_bins[16];  /* rows per numeric bin                             */
-  int32_t rows_redone;   /* FP32_COMP: rows re-accumulated in fp64           */
+  int32_t rows_redone;   /* FP32_COMP: rows accumulated in fp64 instead       */
   int32_t b_sorted;      /* 1 if B rows were found strictly increasing       */
-  double max_row_err;    /* FP32_COMP: largest per-row error bound (relative) */
+  double max_row_err;    /* FP32_COMP: largest per-row error bound of the
+                            fp32-pair rows, relative to sum|a*b|            */
   int32_t launches;      /* kernels this call launched                       */
   float ms_rowinfo;      /* opts.timing: B check + row counts + bins         */
   float ms_symbolic;     /* opts.timing: permutation + symbolic kernels      */
@@ -170,12 +172,15 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip,
                  int64_t *total, void *stream);
 
 /* ---- batched products ------------------------------------------------------ */
-/* `count` independent products C[i] = A[i]·B[i] run through one persistent
- * kernel per phase with a global row work queue across all products. Output
- * arrays are allocated per product with one cudaMalloc each (caller frees).  */
+/* `count` independent products C[i] = A[i]·B[i] run as one block-diagonal
+ * product: one launch per phase and bin over the rows of all products (a
+ * single bin-sorted work queue across products), two host synchronisations
+ * per group of products (groups keep nnz(C) below int32). C[i] are views into
+ * per-group allocations; their base pointers are written to owners (room for
+ * 3*count) and *n_owners; release them with nspb_free.                       */
 int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
-                        nspb_stats *stats);
+                        nspb_stats *stats, void **owners, int32_t *n_owners);
 
 /* ---- column remap (compactcol / getmct) ------------------------------------ */
 /* Sorted unique column indices of col[0..nnz) that fall outside [first,last]

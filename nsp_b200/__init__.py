@@ -31,7 +31,7 @@ def _stream_ptr(stream):
 
 
 def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group_lanes=0,
-              comp_tol=1e-12, stream=None) -> Opts:
+              comp_tol=1e-10, stream=None) -> Opts:
     o = Opts()
     lib.nspb_default_opts(C.byref(o))
     o.precision = precision
@@ -51,7 +51,7 @@ def stats_dict(s: Stats) -> dict:
 
 def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,
            stream=None, check_errors: bool = True, assume_sorted: bool = False,
-           group_lanes: int = 0, comp_tol: float = 1e-12, return_stats: bool = False):
+           group_lanes: int = 0, comp_tol: float = 1e-10, return_stats: bool = False):
     """C = A·B on the current CUDA device through nspb_spgemm.
 
     With `out` given, its tensors are used as C's arrays (capacity = their
@@ -75,6 +75,54 @@ def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR |
         res = DeviceCSR(A.nrows, B.ncols, adopt(c.rowptr, A.nrows + 1, "int32"),
                         adopt(c.col, c.nnz, "int32"), adopt(c.val, c.nnz, "float64"))
     return (res, stats_dict(st)) if return_stats else res
+
+
+def spgemm_batched(As, Bs, precision: str = "fp64", stream=None, return_stats: bool = False):
+    """C[p] = A[p]·B[p] for every pair through nspb_spgemm_batched (one
+    block-diagonal product per group of products). Returns DeviceCSRs whose
+    tensors view the shared output allocations (freed with the last view)."""
+    import torch
+    m = len(As)
+    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    o = make_opts(prec, False, True, 0, 1e-10, stream)
+    a = (CsrIn * m)(*[x.as_in() for x in As])
+    b = (CsrIn * m)(*[x.as_in() for x in Bs])
+    c = (CsrOut * m)()
+    owners = (C.c_void_p * (3 * m + 3))()
+    n_own = C.c_int32(0)
+    st = Stats()
+    check(lib.nspb_spgemm_batched(m, a, b, c, C.byref(o), C.byref(st), owners, C.byref(n_own)),
+          "nspb_spgemm_batched")
+    # one tensor per owner allocation; each product's arrays are slices of them
+    from .csr import DevBuf
+    bases = {}
+    for q in range(n_own.value):
+        bases[owners[q]] = None
+    ptrs = sorted(bases)
+    out = []
+
+    def owner_of(ptr):
+        lo = max(p_ for p_ in ptrs if p_ <= ptr)
+        return lo
+
+    views = {}
+    sizes = {}
+    for p in range(m):
+        for ptr, cnt, es in ((c[p].rowptr, c[p].nrows + 1, 4), (c[p].col, c[p].nnz, 4),
+                             (c[p].val, c[p].nnz, 8)):
+            base = owner_of(ptr)
+            sizes[base] = max(sizes.get(base, 0), ptr - base + cnt * es)
+    for base, nbytes in sizes.items():
+        views[base] = torch.as_tensor(DevBuf(base, nbytes, "|u1"), device="cuda")
+    for p in range(m):
+        def sl(ptr, cnt, dtype):
+            base = owner_of(ptr)
+            raw = views[base][ptr - base: ptr - base + cnt * torch.empty((), dtype=dtype).element_size()]
+            return raw.view(dtype)
+        out.append(DeviceCSR(c[p].nrows, c[p].ncols, sl(c[p].rowptr, c[p].nrows + 1, torch.int32),
+                             sl(c[p].col, c[p].nnz, torch.int32),
+                             sl(c[p].val, c[p].nnz, torch.float64)))
+    return (out, stats_dict(st)) if return_stats else out
 
 
 def spgemm_symbolic(A: DeviceCSR, B: DeviceCSR, stream=None, assume_sorted=False):
@@ -158,3 +206,28 @@ def nsparseMGPU_version1(A: DeviceCSR, B: DeviceCSR):
     res = DeviceCSR(c.M, c.N, adopt(c.d_rpt, c.M + 1, "int32"), adopt(c.d_col, c.nnz, "int32"),
                     adopt(c.d_val, c.nnz, "float64"))
     return res, loc
+
+
+def spgemm_rowblocked(A: DeviceCSR, B: DeviceCSR, budget_bytes: int, stream=None):
+    """C = A·B computed in row blocks whose C fits `budget_bytes` of device
+    memory, written to host arrays; returns (HostCSR, number of blocks)."""
+    import numpy as np
+    from .csr import HostCSR
+    a, b = A.as_in(), B.as_in()
+    o = make_opts(PREC_FP64, False, True, 0, 1e-10, stream)
+    rp = np.empty(A.nrows + 1, dtype=np.int32)
+    nnz = C.c_int64(0)
+    nblk = C.c_int32(0)
+    # size pass: capacity 0 reports nnz(C) through NSPB_ERR_CAPACITY
+    st = lib.nspb_spgemm_rowblocked(C.byref(a), C.byref(b), int(budget_bytes),
+                                    rp.ctypes.data, None, None, 0, C.byref(nnz),
+                                    C.byref(nblk), C.byref(o))
+    if st not in (0, -8):
+        check(st, "nspb_spgemm_rowblocked")
+    col = np.empty(max(nnz.value, 1), dtype=np.int32)
+    val = np.empty(max(nnz.value, 1), dtype=np.float64)
+    check(lib.nspb_spgemm_rowblocked(C.byref(a), C.byref(b), int(budget_bytes), rp.ctypes.data,
+                                     col.ctypes.data, val.ctypes.data, nnz.value, C.byref(nnz),
+                                     C.byref(nblk), C.byref(o)), "nspb_spgemm_rowblocked")
+    n = nnz.value
+    return HostCSR(A.nrows, B.ncols, rp, col[:n], val[:n]), int(nblk.value)

@@ -87,7 +87,8 @@ _SIGS = {
     "nspb_spgemm_symbolic": (C.c_int, [P(CsrIn), P(CsrIn), P(CsrOut), P(Opts), P(Stats)]),
     "nspb_spgemm_numeric": (C.c_int, [P(CsrIn), P(CsrIn), P(CsrOut), P(Opts), P(Stats)]),
     "nspb_intprod": (C.c_int, [P(CsrIn), P(CsrIn), C.c_void_p, P(C.c_int64), C.c_void_p]),
-    "nspb_spgemm_batched": (C.c_int, [C.c_int, P(CsrIn), P(CsrIn), P(CsrOut), P(Opts), P(Stats)]),
+    "nspb_spgemm_batched": (C.c_int, [C.c_int, P(CsrIn), P(CsrIn), P(CsrOut), P(Opts), P(Stats),
+                                      P(C.c_void_p), P(C.c_int32)]),
     "nspb_getmct": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p,
                               P(C.c_int64), C.c_void_p]),
     "nspb_compactcol": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p,

@@ -128,6 +128,50 @@ __device__ __forceinline__ void num_insert(int *keys, double *vals, int key,
   atomicOr(err, ERR_PROBE);
 }
 
+// Slot of `key` in (keys), inserting it when absent; -1 (and the error word)
+// when the probe sequence is exhausted.
+template <int LOG2T>
+__device__ __forceinline__ int num_slot(int *keys, int key, int *err) {
+  constexpr unsigned MASK = (1u << LOG2T) - 1u;
+  unsigned h = hash_slot<LOG2T>(key);
+#pragma unroll 1
+  for (unsigned q = 0; q <= MASK; ++q) {
+    const int cur = ((volatile int *)keys)[h];
+    if (cur == key) return (int)h;
+    if (cur == kEmpty) {
+      const int old = atomicCAS(keys + h, kEmpty, key);
+      if (old == kEmpty || old == key) return (int)h;
+    }
+    h = (h + 1u) & MASK;
+  }
+  atomicOr(err, ERR_PROBE);
+  return -1;
+}
+
+// Error-free fp32 accumulation of a*b into the pair (s, c): TwoProduct by FMA,
+// then TwoSum of s and the high part; the low parts go to c. Rounding is
+// explicit so no step is contracted or reordered.
+__device__ __forceinline__ void comp_add(float2 &sc, float a, float b) {
+  const float ph = __fmul_rn(a, b);
+  const float pl = __fmaf_rn(a, b, -ph);
+  const float t = __fadd_rn(sc.x, ph);
+  const float z = __fsub_rn(t, sc.x);
+  const float e = __fadd_rn(__fsub_rn(sc.x, __fsub_rn(t, z)), __fsub_rn(ph, z));
+  sc.x = t;
+  sc.y = __fadd_rn(sc.y, __fadd_rn(e, pl));
+}
+
+// Value loads as fp64 from fp64 or fp32 arrays (fp32 products are then exact
+// in fp64: 24 + 24 significant bits).
+__device__ __forceinline__ double ldv(const double *p) { return __ldg(p); }
+__device__ __forceinline__ double ldv(const float *p) { return (double)__ldg(p); }
+__device__ __forceinline__ double ldv_stream(const double *p) { return ld_stream(p); }
+__device__ __forceinline__ double ldv_stream(const float *p) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return (double)v;
+}
+
 // Padded index of a bucket counter: one spare slot per 32 counters, so a
 // lane that owns a run of consecutive counters hits its own bank.
 __device__ __forceinline__ int cpad(int b) { return b + (b >> 5); }

@@ -70,15 +70,15 @@ cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
                                const int *rows, int count, int *err,
                                cudaStream_t s);
 
-// ---- fp32c.cu ---------------------------------------------------------------------
-// FP32 compensated numeric phase: fp32 inputs, error-free products and
-// two-sum accumulation, fp64 output, per-row relative error bound written to
-// row_err (bound relative to sum|a*b|). Rows flagged in redo get fp64 values.
-cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool b_sorted,
-                                    const CsrDev &A, const CsrDev &B,
-                                    const int *crpt, int *ccol, double *cval,
-                                    const int *rows, int count, double tol,
-                                    int *redo_rows, int *redo_count,
-                                    float *row_err, int *err, cudaStream_t s);
+// Compensated numeric step (fp32 inputs): rows with at most nmax A entries
+// accumulate error-free fp32 pairs (TwoProduct + TwoSum) collapsed to fp64;
+// the other rows accumulate fp64 products of the widened inputs. *redo
+// counts the fp64 rows, *max_deg receives the largest A-row degree among the
+// pair rows.
+cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorted,
+                                    const CsrDev &A, const CsrDev &B, const int *crpt,
+                                    int *ccol, double *cval, const int *rows, int count,
+                                    int nmax, int *redo, int *max_deg, int *err,
+                                    cudaStream_t s);
 
 }  // namespace nspb

@@ -39,14 +39,24 @@ struct NumGroupCfg {
   static constexpr int PER = NB >= G ? NB / G : 1;  // scan counters per lane
 };
 
-template <int G, int LOG2T, bool OWNED>
+// Compensated-mode parameters of a numeric launch (fp32 inputs).
+struct CompArgs {
+  int nmax;        // rows with at most nmax A entries accumulate error-free in
+                   // fp32 pairs; longer rows accumulate in fp64
+  int *redo;       // counter of rows accumulated in fp64
+  int *max_deg;    // largest A-row degree among the pair-accumulated rows
+};
+
+// VT: value type of A and B (double, or float in the compensated mode).
+// COMP: fp32 inputs with the error-free pair accumulation for short rows.
+template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>
 __global__ void __launch_bounds__(256)
     k_num_group(const int *__restrict__ arpt, const int *__restrict__ acol,
-                const double *__restrict__ aval, const int *__restrict__ brpt,
-                const int *__restrict__ bcol, const double *__restrict__ bval,
+                const VT *__restrict__ aval, const int *__restrict__ brpt,
+                const int *__restrict__ bcol, const VT *__restrict__ bval,
                 const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
-                int *__restrict__ err) {
+                int *__restrict__ err, CompArgs comp) {
   using C = NumGroupCfg<G, LOG2T>;
   extern __shared__ __align__(16) unsigned char smem_num[];
   auto tile = cg::tiled_partition<G>(cg::this_thread_block());
@@ -68,13 +78,16 @@ __global__ void __launch_bounds__(256)
     }
     tile.sync();
     const int a0 = arpt[row], a1 = arpt[row + 1];
+    // compensated mode: pair accumulation when the row's Dot2 bound allows it
+    const bool pair = COMP && OWNED && (a1 - a0) <= comp.nmax;
+    float2 *vals2 = reinterpret_cast<float2 *>(vals);
     int mn = 0x7fffffff, mx = -1;
     for (int ab = a0; ab < a1; ab += G) {
       int bs = 0, be = 0;
       double av = 0.0;
       if (ab + lane < a1) {
         const int k = ld_stream(acol + ab + lane);
-        av = ld_stream(aval + ab + lane);
+        av = ldv_stream(aval + ab + lane);
         bs = __ldg(brpt + k);
         be = __ldg(brpt + k + 1);
       }
@@ -86,8 +99,16 @@ __global__ void __launch_bounds__(256)
           const int e = base + lane;
           if (e < s1) {
             const int key = __ldg(bcol + e);
-            const double p = __dmul_rn(a, __ldg(bval + e));
-            num_insert<LOG2T, OWNED>(keys, vals, key, p, err);
+            if (pair) {
+              const int h = num_slot<LOG2T>(keys, key, err);
+              if (h >= 0) {
+                float2 sc = vals2[h];
+                comp_add(sc, (float)a, __ldg(reinterpret_cast<const float *>(bval) + e));
+                vals2[h] = sc;
+              }
+            } else {
+              num_insert<LOG2T, OWNED>(keys, vals, key, __dmul_rn(a, ldv(bval + e)), err);
+            }
             mn = min(mn, key);
             mx = max(mx, key);
           }
@@ -96,6 +117,21 @@ __global__ void __launch_bounds__(256)
       }
     }
     tile.sync();
+    if (COMP) {
+      if (pair) {  // collapse each (s, c) pair to fp64
+        for (int s = lane; s < C::T; s += G) {
+          if (keys[s] >= 0) {
+            const float2 sc = vals2[s];
+            vals[s] = (double)sc.x + (double)sc.y;
+          }
+        }
+        const int deg = cg::reduce(tile, a1 - a0, cg::greater<int>());
+        if (lane == 0) atomicMax(comp.max_deg, deg);
+      } else if (lane == 0) {
+        atomicAdd(comp.redo, 1);
+      }
+      tile.sync();
+    }
     const int c0 = crpt[row];
     const int n = crpt[row + 1] - c0;
     mn = cg::reduce(tile, mn, cg::less<int>());
@@ -189,14 +225,14 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *red, int *tot) {
   return r;
 }
 
-template <int LOG2T>
+template <int LOG2T, typename VT>
 __global__ void __launch_bounds__(kNumBlockThreads)
     k_num_block(const int *__restrict__ arpt, const int *__restrict__ acol,
-                const double *__restrict__ aval, const int *__restrict__ brpt,
-                const int *__restrict__ bcol, const double *__restrict__ bval,
+                const VT *__restrict__ aval, const int *__restrict__ brpt,
+                const int *__restrict__ bcol, const VT *__restrict__ bval,
                 const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
-                int *__restrict__ err) {
+                int *__restrict__ err, int *__restrict__ redo) {
   constexpr int T = 1 << LOG2T, H = T / 2, NB = T / 2;
   constexpr int PER = NB / kNumBlockThreads;
   extern __shared__ __align__(16) unsigned char smem_num[];
@@ -225,11 +261,11 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     int mn = 0x7fffffff, mx = -1;
     for (int j = a0 + warp; j < a1; j += W) {
       const int k = ld_stream(acol + j);
-      const double a = ld_stream(aval + j);
+      const double a = ldv_stream(aval + j);
       const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
       for (int e = s0 + lane; e < s1; e += 32) {
         const int key = __ldg(bcol + e);
-        num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, __ldg(bval + e)), err);
+        num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, ldv(bval + e)), err);
         mn = min(mn, key);
         mx = max(mx, key);
       }
@@ -243,6 +279,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
       atomicMin(&s_mn, mn);
       atomicMax(&s_mx, mx);
     }
+    if (redo && threadIdx.x == 0) atomicAdd(redo, 1);  // compensated mode: an fp64 row
     __syncthreads();
     mn = s_mn;
     mx = s_mx;
@@ -314,13 +351,15 @@ __device__ __forceinline__ int lower_bound_col(const int *__restrict__ col, int 
   return lo;
 }
 
+template <typename VT>
 __global__ void __launch_bounds__(kNumLongThreads)
     k_num_long(const int *__restrict__ arpt, const int *__restrict__ acol,
-               const double *__restrict__ aval, const int *__restrict__ brpt,
-               const int *__restrict__ bcol, const double *__restrict__ bval,
+               const VT *__restrict__ aval, const int *__restrict__ brpt,
+               const int *__restrict__ bcol, const VT *__restrict__ bval,
                int ncols, bool sorted, const int *__restrict__ crpt,
                int *__restrict__ ccol, double *__restrict__ cval,
-               const int *__restrict__ rows, int count, int *__restrict__ err) {
+               const int *__restrict__ rows, int count, int *__restrict__ err,
+               int *__restrict__ redo) {
   extern __shared__ __align__(16) unsigned char smem_num[];
   double *dense = reinterpret_cast<double *>(smem_num);
   unsigned *bm = reinterpret_cast<unsigned *>(dense + kWin);
@@ -341,7 +380,7 @@ __global__ void __launch_bounds__(kNumLongThreads)
       if (per_thread) {  // one A entry per thread
         for (int j = a0 + threadIdx.x; j < a1; j += kNumLongThreads) {
           const int k = ld_stream(acol + j);
-          const double a = ld_stream(aval + j);
+          const double a = ldv_stream(aval + j);
           const int s1 = __ldg(brpt + k + 1);
           int e = __ldg(brpt + k);
           if (sorted) e = lower_bound_col(bcol, e, s1, w0);
@@ -350,7 +389,7 @@ __global__ void __launch_bounds__(kNumLongThreads)
             if (sorted && c >= w1) break;
             const unsigned d = (unsigned)(c - w0);
             if (d < (unsigned)kWin) {
-              atomicAdd(dense + d, __dmul_rn(a, __ldg(bval + e)));
+              atomicAdd(dense + d, __dmul_rn(a, ldv(bval + e)));
               const unsigned bit = 1u << (d & 31u);
               if (!(bm[d >> 5] & bit)) atomicOr(bm + (d >> 5), bit);
             }
@@ -359,7 +398,7 @@ __global__ void __launch_bounds__(kNumLongThreads)
       } else {  // one A entry per warp, lanes over the B row
         for (int j = a0 + warp; j < a1; j += W) {
           const int k = ld_stream(acol + j);
-          const double a = ld_stream(aval + j);
+          const double a = ldv_stream(aval + j);
           const int s1 = __ldg(brpt + k + 1);
           int e0 = __ldg(brpt + k);
           if (sorted) e0 = lower_bound_col(bcol, e0, s1, w0);
@@ -368,7 +407,7 @@ __global__ void __launch_bounds__(kNumLongThreads)
             if (sorted && c >= w1) break;
             const unsigned d = (unsigned)(c - w0);
             if (d < (unsigned)kWin) {
-              atomicAdd(dense + d, __dmul_rn(a, __ldg(bval + e)));
+              atomicAdd(dense + d, __dmul_rn(a, ldv(bval + e)));
               const unsigned bit = 1u << (d & 31u);
               if (!(bm[d >> 5] & bit)) atomicOr(bm + (d >> 5), bit);
             }
@@ -416,49 +455,93 @@ __global__ void __launch_bounds__(kNumLongThreads)
       __syncthreads();
     }
     if (threadIdx.x == 0 && off != row_end) atomicOr(err, ERR_COUNT);
+    if (redo && threadIdx.x == 0) atomicAdd(redo, 1);  // compensated mode: an fp64 row
   }
 }
 
 // ---- dispatch ------------------------------------------------------------------------
-template <int G, int LOG2T, bool OWNED>
-static cudaError_t run_num_group(const CsrDev &A, const CsrDev &B, const int *crpt, int *ccol,
-                                 double *cval, const int *rows, int count, int *err,
-                                 cudaStream_t s) {
+template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>
+static cudaError_t run_num_group(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
+                                 const int *crpt, int *ccol, double *cval, const int *rows,
+                                 int count, int *err, CompArgs comp, cudaStream_t s) {
   using C = NumGroupCfg<G, LOG2T>;
-  const void *f = (const void *)k_num_group<G, LOG2T, OWNED>;
+  const void *f = (const void *)k_num_group<G, LOG2T, OWNED, VT, COMP>;
   const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_group<G, LOG2T, OWNED><<<grid, C::THREADS, C::SMEM, s>>>(
-      A.rpt, A.col, A.val, B.rpt, B.col, B.val, crpt, ccol, cval, rows, count, err);
+  k_num_group<G, LOG2T, OWNED, VT, COMP><<<grid, C::THREADS, C::SMEM, s>>>(
+      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, comp);
   return cudaGetLastError();
 }
 
-template <int G, bool OWNED>
-static cudaError_t num_group_bin(int bin, const CsrDev &A, const CsrDev &B, const int *crpt,
-                                 int *ccol, double *cval, const int *rows, int count,
-                                 int *err, cudaStream_t s) {
+template <int G, bool OWNED, typename VT, bool COMP>
+static cudaError_t num_group_bin(int bin, const CsrDev &A, const CsrDev &B, const VT *av,
+                                 const VT *bv, const int *crpt, int *ccol, double *cval,
+                                 const int *rows, int count, int *err, CompArgs comp,
+                                 cudaStream_t s) {
+#define NSPB_NG(L2T) \
+  run_num_group<G, L2T, OWNED, VT, COMP>(A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
   switch (bin) {
-    case 0: return run_num_group<G, 5, OWNED>(A, B, crpt, ccol, cval, rows, count, err, s);
-    case 1: return run_num_group<G, 6, OWNED>(A, B, crpt, ccol, cval, rows, count, err, s);
-    case 2: return run_num_group<G, 7, OWNED>(A, B, crpt, ccol, cval, rows, count, err, s);
-    case 3: return run_num_group<G, 8, OWNED>(A, B, crpt, ccol, cval, rows, count, err, s);
-    case 4: return run_num_group<G, 9, OWNED>(A, B, crpt, ccol, cval, rows, count, err, s);
-    default: return run_num_group<G, 10, OWNED>(A, B, crpt, ccol, cval, rows, count, err, s);
+    case 0: return NSPB_NG(5);
+    case 1: return NSPB_NG(6);
+    case 2: return NSPB_NG(7);
+    case 3: return NSPB_NG(8);
+    case 4: return NSPB_NG(9);
+    default: return NSPB_NG(10);
   }
+#undef NSPB_NG
 }
 
-template <int LOG2T>
-static cudaError_t run_num_block(const CsrDev &A, const CsrDev &B, const int *crpt, int *ccol,
-                                 double *cval, const int *rows, int count, int *err,
-                                 cudaStream_t s) {
+template <int LOG2T, typename VT>
+static cudaError_t run_num_block(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
+                                 const int *crpt, int *ccol, double *cval, const int *rows,
+                                 int count, int *err, int *redo, cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
   const int smem = T * 12 + (T / 2) * 12 + (T / 2) * 4;
-  const void *f = (const void *)k_num_block<LOG2T>;
+  const void *f = (const void *)k_num_block<LOG2T, VT>;
   const int grid = persistent_grid(f, kNumBlockThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_block<LOG2T><<<grid, kNumBlockThreads, smem, s>>>(
-      A.rpt, A.col, A.val, B.rpt, B.col, B.val, crpt, ccol, cval, rows, count, err);
+  k_num_block<LOG2T, VT><<<grid, kNumBlockThreads, smem, s>>>(
+      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, redo);
   return cudaGetLastError();
+}
+
+template <typename VT, bool COMP>
+static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, const CsrDev &A,
+                                 const CsrDev &B, const VT *av, const VT *bv, const int *crpt,
+                                 int *ccol, double *cval, const int *rows, int count, int *err,
+                                 CompArgs comp, cudaStream_t s) {
+  if (bin < kNumGroupBins) {
+#define NSPB_GB(GL, OW) \
+  num_group_bin<GL, OW, VT, COMP>(bin, A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
+    if (owned) {
+      if (lanes == 8) return NSPB_GB(8, true);
+      if (lanes == 16) return NSPB_GB(16, true);
+      return NSPB_GB(32, true);
+    }
+    if (lanes == 8) return NSPB_GB(8, false);
+    if (lanes == 16) return NSPB_GB(16, false);
+    return NSPB_GB(32, false);
+#undef NSPB_GB
+  }
+  int *redo = COMP ? comp.redo : nullptr;
+  switch (bin) {
+    case kNumGroupBins:
+      return run_num_block<11, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
+    case kNumGroupBins + 1:
+      return run_num_block<12, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
+    case kNumGroupBins + 2:
+      return run_num_block<13, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
+    default: {
+      const int smem = kWin * 8 + kWinWords * 4;
+      const void *f = (const void *)k_num_long<VT>;
+      const int grid = persistent_grid(f, kNumLongThreads, smem, count, 1);
+      if (grid <= 0) return cudaErrorInvalidConfiguration;
+      k_num_long<VT><<<grid, kNumLongThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv,
+                                                         B.ncols, b_sorted, crpt, ccol, cval,
+                                                         rows, count, err, redo);
+      return cudaGetLastError();
+    }
+  }
 }
 
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
@@ -466,31 +549,20 @@ cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
                                int *ccol, double *cval, const int *rows, int count,
                                int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  if (bin < kNumGroupBins) {
-    if (owned) {
-      if (lanes == 8) return num_group_bin<8, true>(bin, A, B, crpt, ccol, cval, rows, count, err, s);
-      if (lanes == 16) return num_group_bin<16, true>(bin, A, B, crpt, ccol, cval, rows, count, err, s);
-      return num_group_bin<32, true>(bin, A, B, crpt, ccol, cval, rows, count, err, s);
-    }
-    if (lanes == 8) return num_group_bin<8, false>(bin, A, B, crpt, ccol, cval, rows, count, err, s);
-    if (lanes == 16) return num_group_bin<16, false>(bin, A, B, crpt, ccol, cval, rows, count, err, s);
-    return num_group_bin<32, false>(bin, A, B, crpt, ccol, cval, rows, count, err, s);
-  }
-  switch (bin) {
-    case kNumGroupBins: return run_num_block<11>(A, B, crpt, ccol, cval, rows, count, err, s);
-    case kNumGroupBins + 1: return run_num_block<12>(A, B, crpt, ccol, cval, rows, count, err, s);
-    case kNumGroupBins + 2: return run_num_block<13>(A, B, crpt, ccol, cval, rows, count, err, s);
-    default: {
-      const int smem = kWin * 8 + kWinWords * 4;
-      const void *f = (const void *)k_num_long;
-      const int grid = persistent_grid(f, kNumLongThreads, smem, count, 1);
-      if (grid <= 0) return cudaErrorInvalidConfiguration;
-      k_num_long<<<grid, kNumLongThreads, smem, s>>>(A.rpt, A.col, A.val, B.rpt, B.col, B.val,
-                                                     B.ncols, b_sorted, crpt, ccol, cval, rows,
-                                                     count, err);
-      return cudaGetLastError();
-    }
-  }
+  return numeric_bin_t<double, false>(bin, lanes, owned, b_sorted, A, B, A.val, B.val, crpt,
+                                      ccol, cval, rows, count, err, CompArgs{0, nullptr, nullptr},
+                                      s);
+}
+
+cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorted,
+                                    const CsrDev &A, const CsrDev &B, const int *crpt,
+                                    int *ccol, double *cval, const int *rows, int count,
+                                    int nmax, int *redo, int *max_deg, int *err,
+                                    cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  return numeric_bin_t<float, true>(bin, lanes, owned, b_sorted, A, B, A.val32, B.val32, crpt,
+                                    ccol, cval, rows, count, err, CompArgs{nmax, redo, max_deg},
+                                    s);
 }
 
 }  // namespace nspb

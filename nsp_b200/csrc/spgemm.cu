@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -281,11 +282,16 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
       return cuda_fail(e);
     ++launches;
   }
+  const bool comp = opts.precision == NSPB_PREC_FP32_COMP;
+  const int nmax = comp ? comp_nmax(opts.comp_tol) : 0;
   for (int b = 0; b < kNumBins; ++b) {
     const int c = h.num_counts[b];
     if (c <= 0) continue;
-    e = launch_numeric_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval,
-                           direct ? nullptr : perm + off.v[b], c, &ctr->err, s);
+    const int *rows = direct ? nullptr : perm + off.v[b];
+    e = comp ? launch_numeric_comp_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows,
+                                       c, nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
+             : launch_numeric_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows, c,
+                                  &ctr->err, s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
@@ -309,8 +315,23 @@ int Call::prepare_numeric(const int *crpt) {
   return NSPB_OK;
 }
 
+// Largest A-row degree n whose Dot2 error bound gamma_n^2 (gamma_n =
+// n u / (1 - n u), u = 2^-24, Ogita, Rump and Oishi 2005) stays within tol,
+// relative to sum |a_ik b_kj|; fp32 pairs then add within tol of the exact sum.
+int comp_nmax(double tol) {
+  if (!(tol > 0.0)) tol = 1e-10;
+  const double u = 0x1.0p-24, r = std::sqrt(tol);
+  return (int)std::floor(r / (u * (1.0 + r)));
+}
+
+double comp_bound(int n) {
+  if (n <= 0) return 0.0;
+  const double u = 0x1.0p-24, g = n * u / (1.0 - n * u);
+  return g * g + 0x1.0p-53;
+}
+
 int Call::finish(nspb_stats *stats) {
-  if (opts.check_errors && n > 0) {
+  if ((opts.check_errors || opts.precision == NSPB_PREC_FP32_COMP) && n > 0) {
     int st = fetch_counters();
     if (st) return st;
   }
@@ -322,6 +343,8 @@ int Call::finish(nspb_stats *stats) {
       stats->num_bins[b] = b < kNumBins ? h.num_counts[b] : 0;
     }
     stats->b_sorted = b_sorted ? 1 : 0;
+    stats->rows_redone = opts.precision == NSPB_PREC_FP32_COMP ? h.redo_count : 0;
+    stats->max_row_err = opts.precision == NSPB_PREC_FP32_COMP ? comp_bound(h.max_comp_deg) : 0.0;
     stats->launches = launches;
     stats->ms_rowinfo = stats->ms_symbolic = stats->ms_scan = stats->ms_numeric = 0.f;
     if (timing && n > 0) {
@@ -382,7 +405,7 @@ void nspb_default_opts(nspb_opts *o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
   o->precision = NSPB_PREC_FP64;
-  o->comp_tol = 1e-12;
+  o->comp_tol = 1e-10;
 }
 
 int nspb_free(void *p) {

@@ -23,7 +23,8 @@ struct DevCounters {
   unsigned long long total_ip;
   long long total_nnz;
   float max_row_err;
-  int pad[3];
+  int max_comp_deg;  // compensated mode: largest A-row degree of a pair row
+  int pad[2];
 };
 
 struct HostStage {
@@ -81,5 +82,9 @@ struct Call {
 
 // Numeric step in the call's precision mode (fp64 or fp32-compensated).
 int run_numeric_mode(Call &call, nspb_csr_out *C);
+// Compensated mode: longest A row accumulated in fp32 pairs for a tolerance,
+// and the relative error bound of a pair row with n A entries.
+int comp_nmax(double tol);
+double comp_bound(int n);
 
 }  // namespace nspb

@@ -46,7 +46,7 @@ def test_strerror_and_defaults():
     assert b"int32" in nb.lib.nspb_strerror(_lib.ERR_OVERFLOW)
     o = _lib.Opts()
     nb.lib.nspb_default_opts(ctypes.byref(o))
-    assert o.precision == _lib.PREC_FP64 and o.comp_tol == 1e-12
+    assert o.precision == _lib.PREC_FP64 and o.comp_tol == 1e-10
 
 
 def test_generator_thread_independent():
