@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--grid", type=int, default=128,
                    help="stencil edge L (default 128; smaller grids for profiler captures)")
     p.add_argument("--workload", default="stencil27",
-                   choices=["stencil27", "amg_batch", "fp32c"],
+                   choices=["stencil27", "amg_batch", "fp32c", "powerlaw"],
                    help="stencil27: the headline line; amg_batch: batched vs one call per "
                         "product; fp32c: compensated fp32 vs fp64 on the 27-point stencil")
     p.add_argument("--batch-count", type=int, default=256)
@@ -131,6 +131,37 @@ def run_amg_batch(args):
                      "batched_gflops": 2 * ip_amg / ms_ba / 1e6, "batched_ms": ms_ba,
                      "one_call_gflops": 2 * ip_amg / ms_sa / 1e6, "one_call_ms": ms_sa}}),
         flush=True)
+
+
+def run_powerlaw(args):
+    """C = A·A for the power-law matrix (n = 1M, Zipf alpha 2.1, mean degree
+    16, max 50k): every bin, including the long-row kernels."""
+    import torch
+    import nsp_b200 as nb
+    P = nb.gen.powerlaw(1_000_000, alpha=2.1, mean_deg=16.0, max_deg=50_000, seed=SEED)
+    dP = P.to_device()
+    C0, st0 = nb.spgemm(dP, dP, return_stats=True)
+    nnz = st0["nnz"]
+    del C0
+    out = nb.DeviceCSR(P.nrows, P.ncols, torch.empty(P.nrows + 1, dtype=torch.int32, device="cuda"),
+                       torch.empty(nnz, dtype=torch.int32, device="cuda"),
+                       torch.empty(nnz, dtype=torch.float64, device="cuda"))
+    phases = {}
+
+    def step():
+        _, s = nb.spgemm(dP, dP, out=out, check_errors=False, return_stats=True)
+
+    ms = _timed(step, args.steps, max(args.warmup, 1))
+    _, st = nb.spgemm(dP, dP, out=out, return_stats=True)
+    print(json.dumps({
+        "metric": "SpGEMM GFLOP/s, C=A*A, power-law n=1M (alpha 2.1, mean 16, max 50k), fp64",
+        "value": 2 * st0["intprod"] / ms / 1e6, "unit": "GFLOP/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "f64", "data": f"synthetic (seed {SEED})",
+        "config": {"workload": "powerlaw_1M_AxA_fp64", "nnz_A": P.nnz,
+                   "xmin": nb.gen.powerlaw_xmin(), "intprod": st0["intprod"], "nnz_C": nnz,
+                   "sym_bins": st["sym_bins"], "num_bins": st["num_bins"]},
+        "effective_gbs": alg_bytes(P, P, nnz) / (ms * 1e-3) / 1e9}), flush=True)
 
 
 def run_fp32c(args):
@@ -345,6 +376,8 @@ def main():
         return run_amg_batch(args)
     if args.workload == "fp32c":
         return run_fp32c(args)
+    if args.workload == "powerlaw":
+        return run_powerlaw(args)
 
     import ctypes as C
     import torch

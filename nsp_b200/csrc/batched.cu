@@ -34,73 +34,45 @@ struct CatDesc {
   int col_shift;      // added to every column of this block
 };
 
-// Index of the block holding item t: largest p with off[p] <= t.
-__device__ __forceinline__ int block_of(const long long *off, int m, long long t) {
-  int lo = 0, hi = m - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (off[mid] <= t) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
+// The concatenation and split kernels run on a 2-D grid: blockIdx.y is the
+// product, blockIdx.x strides over that product's rows or entries, so no item
+// has to search for its product.
 template <typename VT>
-__global__ void k_cat_entries(const CatDesc *__restrict__ d, const long long *__restrict__ nnz_off,
-                              int m, long long total, int *__restrict__ col,
+__global__ void k_cat_entries(const CatDesc *__restrict__ d, int *__restrict__ col,
                               VT *__restrict__ val) {
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int p = block_of(nnz_off, m, t);
-    const CatDesc &q = d[p];
-    const long long e = t - q.nnz_off + q.rpt[0];
-    col[t] = q.col[e] + q.col_shift;
-    val[t] = static_cast<const VT *>(q.val)[e];
+  const CatDesc q = d[blockIdx.y];
+  const long long n = (long long)(q.nrows > 0 ? q.rpt[q.nrows] - q.rpt[0] : 0);
+  const long long e0 = q.nrows > 0 ? q.rpt[0] : 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    col[q.nnz_off + e] = q.col[e0 + e] + q.col_shift;
+    val[q.nnz_off + e] = static_cast<const VT *>(q.val)[e0 + e];
   }
 }
 
-__global__ void k_cat_rows(const CatDesc *__restrict__ d, const long long *__restrict__ row_off,
-                           int m, long long total, long long nnz_total, int *__restrict__ rpt) {
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g <= total;
-       g += (long long)gridDim.x * blockDim.x) {
-    if (g == total) {  // blocks with no rows may have no row pointer at all
-      rpt[g] = (int)nnz_total;
-      continue;
-    }
-    const int p = block_of(row_off, m, g);
-    const CatDesc &q = d[p];
-    const long long i = g - q.row_off;
-    rpt[g] = (int)(q.nnz_off + (q.rpt[i] - q.rpt[0]));
-  }
+__global__ void k_cat_rows(const CatDesc *__restrict__ d, long long total, long long nnz_total,
+                           int *__restrict__ rpt) {
+  const CatDesc q = d[blockIdx.y];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < q.nrows;
+       i += (long long)gridDim.x * blockDim.x)
+    rpt[q.row_off + i] = (int)(q.nnz_off + (q.rpt[i] - q.rpt[0]));
+  if (blockIdx.y == 0 && blockIdx.x == 0 && threadIdx.x == 0) rpt[total] = (int)nnz_total;
 }
 
 // Per-product row pointers (product p's at out_rpt + row_off[p] + p) and the
 // column shift undone in place.
 __global__ void k_split(const int *__restrict__ crpt, const long long *__restrict__ row_off,
-                        const int *__restrict__ shift, int m, long long rows_total,
-                        int *__restrict__ out_rpt, int *__restrict__ ccol,
-                        long long nnz_total) {
-  const long long n_rp = rows_total + m;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n_rp;
-       t += (long long)gridDim.x * blockDim.x) {
-    // t indexes the concatenation of per-product row pointers (n_p + 1 each)
-    int lo = 0, hi = m - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (row_off[mid] + mid <= t) lo = mid; else hi = mid - 1;
-    }
-    const long long i = t - (row_off[lo] + lo);
-    out_rpt[t] = crpt[row_off[lo] + i] - crpt[row_off[lo]];
-  }
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nnz_total;
-       t += (long long)gridDim.x * blockDim.x) {
-    // the block of entry t: rows are ordered, so search the row pointer bounds
-    int lo = 0, hi = m - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (crpt[row_off[mid]] <= t) lo = mid; else hi = mid - 1;
-    }
-    ccol[t] -= shift[lo];
-  }
+                        const int *__restrict__ shift, int *__restrict__ out_rpt,
+                        int *__restrict__ ccol) {
+  const int p = blockIdx.y;
+  const long long r0 = row_off[p], n = row_off[p + 1] - r0;
+  const int c0 = crpt[r0], c1 = crpt[r0 + n], sh = shift[p];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (long long)gridDim.x * blockDim.x)
+    out_rpt[r0 + p + i] = crpt[r0 + i] - c0;
+  for (long long t = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < c1;
+       t += (long long)gridDim.x * blockDim.x)
+    ccol[t] -= sh;
 }
 
 // starts[p] = crpt[row_off[p]] for p <= m (row_off[m] = all rows).
@@ -108,6 +80,14 @@ __global__ void k_gather_starts(const int *__restrict__ crpt, const long long *_
                                 int m, int *__restrict__ starts) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= m; p += gridDim.x * blockDim.x)
     starts[p] = crpt[row_off[p]];
+}
+
+// Blocks per product on the x axis of the 2-D grids: enough to fill the GPU
+// for the largest product of the group.
+static dim3 grid2(long long largest, int m) {
+  long long g = (largest + 255) / 256;
+  const long long cap = std::max<long long>(1, (long long)dev_info().sms * 8);
+  return dim3((unsigned)std::max<long long>(1, std::min(g, cap)), (unsigned)m);
 }
 
 static int grid_cap(long long n) {
@@ -194,18 +174,22 @@ static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, 
   int *brp = reinterpret_cast<int *>(D(o_brp)), *bcl = reinterpret_cast<int *>(D(o_bcl));
   int *crp = reinterpret_cast<int *>(D(o_crp));
   const long long *d_ar = reinterpret_cast<const long long *>(D(o_ar));
-  const long long *d_an = reinterpret_cast<const long long *>(D(o_an));
-  const long long *d_br = reinterpret_cast<const long long *>(D(o_br));
-  const long long *d_bn = reinterpret_cast<const long long *>(D(o_bn));
   if (e == cudaSuccess) {
-    k_cat_rows<<<grid_cap(rows_a + 1), 256, 0, s>>>(dda, d_ar, count, rows_a, nnz_a, arp);
-    k_cat_rows<<<grid_cap(rows_b + 1), 256, 0, s>>>(ddb, d_br, count, rows_b, nnz_b, brp);
+    long long max_ra = 0, max_rb = 0, max_na = 0, max_nb = 0;
+    for (int p = 0; p < count; ++p) {
+      max_ra = std::max<long long>(max_ra, A[p].nrows);
+      max_rb = std::max<long long>(max_rb, B[p].nrows);
+      max_na = std::max<long long>(max_na, A[p].nnz);
+      max_nb = std::max<long long>(max_nb, B[p].nnz);
+    }
+    k_cat_rows<<<grid2(max_ra, count), 256, 0, s>>>(dda, rows_a, nnz_a, arp);
+    k_cat_rows<<<grid2(max_rb, count), 256, 0, s>>>(ddb, rows_b, nnz_b, brp);
     if (f32) {
-      if (nnz_a) k_cat_entries<float><<<grid_cap(nnz_a), 256, 0, s>>>(dda, d_an, count, nnz_a, acl, reinterpret_cast<float *>(D(o_avl)));
-      if (nnz_b) k_cat_entries<float><<<grid_cap(nnz_b), 256, 0, s>>>(ddb, d_bn, count, nnz_b, bcl, reinterpret_cast<float *>(D(o_bvl)));
+      k_cat_entries<float><<<grid2(max_na, count), 256, 0, s>>>(dda, acl, reinterpret_cast<float *>(D(o_avl)));
+      k_cat_entries<float><<<grid2(max_nb, count), 256, 0, s>>>(ddb, bcl, reinterpret_cast<float *>(D(o_bvl)));
     } else {
-      if (nnz_a) k_cat_entries<double><<<grid_cap(nnz_a), 256, 0, s>>>(dda, d_an, count, nnz_a, acl, reinterpret_cast<double *>(D(o_avl)));
-      if (nnz_b) k_cat_entries<double><<<grid_cap(nnz_b), 256, 0, s>>>(ddb, d_bn, count, nnz_b, bcl, reinterpret_cast<double *>(D(o_bvl)));
+      k_cat_entries<double><<<grid2(max_na, count), 256, 0, s>>>(dda, acl, reinterpret_cast<double *>(D(o_avl)));
+      k_cat_entries<double><<<grid2(max_nb, count), 256, 0, s>>>(ddb, bcl, reinterpret_cast<double *>(D(o_bvl)));
     }
     e = cudaGetLastError();
   }
@@ -233,9 +217,10 @@ static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, 
   int *rp_all = nullptr;
   st = alloc_out(reinterpret_cast<void **>(&rp_all), 4 * (size_t)(rows_a + count));
   if (!st) {
-    k_split<<<grid_cap(std::max<long long>(rows_a + count, Ccat.nnz)), 256, 0, s>>>(
-        crp, d_ar, reinterpret_cast<const int *>(D(o_sh)), count, rows_a, rp_all, Ccat.col,
-        Ccat.nnz);
+    // the largest product's C bounds the x extent (its rows and entries)
+    const long long per = std::max<long long>(Ccat.nnz / std::max(count, 1) * 4, 1 << 16);
+    k_split<<<grid2(per, count), 256, 0, s>>>(crp, d_ar, reinterpret_cast<const int *>(D(o_sh)),
+                                               rp_all, Ccat.col);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
       g_last_cuda = (int)e;

@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(256)
   int *bkeys = keys + C::T;
   int *cnt = bkeys + C::H;
 
+  int my_max_deg = 0, my_redo = 0;  // compensated mode, flushed once per group
   for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
     const int row = rows ? rows[r] : r;
 #pragma unroll 4
@@ -125,10 +126,9 @@ __global__ void __launch_bounds__(256)
             vals[s] = (double)sc.x + (double)sc.y;
           }
         }
-        const int deg = cg::reduce(tile, a1 - a0, cg::greater<int>());
-        if (lane == 0) atomicMax(comp.max_deg, deg);
-      } else if (lane == 0) {
-        atomicAdd(comp.redo, 1);
+        my_max_deg = max(my_max_deg, a1 - a0);
+      } else {
+        ++my_redo;
       }
       tile.sync();
     }
@@ -192,6 +192,10 @@ __global__ void __launch_bounds__(256)
     }
     tile.sync();
   }
+  if (COMP && lane == 0) {
+    if (my_max_deg) atomicMax(comp.max_deg, my_max_deg);
+    if (my_redo) atomicAdd(comp.redo, my_redo);
+  }
 }
 
 // ---- block per row: warps over A entries, atomic accumulation ----------------------
@@ -245,6 +249,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
   __shared__ int s_mn, s_mx;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int W = kNumBlockThreads / 32;
+  int rows_done = 0;
   for (int r = blockIdx.x; r < count; r += gridDim.x) {
     const int row = rows ? rows[r] : r;
     for (int s = threadIdx.x; s < T; s += kNumBlockThreads) {
@@ -279,7 +284,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
       atomicMin(&s_mn, mn);
       atomicMax(&s_mx, mx);
     }
-    if (redo && threadIdx.x == 0) atomicAdd(redo, 1);  // compensated mode: an fp64 row
+    ++rows_done;  // compensated mode: every row here is an fp64 row
     __syncthreads();
     mn = s_mn;
     mx = s_mx;
@@ -336,6 +341,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     }
     __syncthreads();
   }
+  if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
 }
 
 // ---- longest rows: dense column windows in shared memory ----------------------------
@@ -366,6 +372,7 @@ __global__ void __launch_bounds__(kNumLongThreads)
   __shared__ int red[kNumLongThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int W = kNumLongThreads / 32;
+  int rows_done = 0;
   for (int r = blockIdx.x; r < count; r += gridDim.x) {
     const int row = rows ? rows[r] : r;
     const int a0 = arpt[row], a1 = arpt[row + 1];
@@ -455,8 +462,9 @@ __global__ void __launch_bounds__(kNumLongThreads)
       __syncthreads();
     }
     if (threadIdx.x == 0 && off != row_end) atomicOr(err, ERR_COUNT);
-    if (redo && threadIdx.x == 0) atomicAdd(redo, 1);  // compensated mode: an fp64 row
+    ++rows_done;  // compensated mode: every row here is an fp64 row
   }
+  if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
 }
 
 // ---- dispatch ------------------------------------------------------------------------

@@ -88,14 +88,14 @@ def spgemm(A, B, nthreads=0):
     columns, kept zeros, fp64 sums of rounded products in A-row order."""
     rp = symbolic(A, B, nthreads)
     nnz = int(rp[-1])
-    col = np.empty(nnz, dtype=np.int32)
-    val = np.empty(nnz, dtype=np.float64)
+    col = np.empty(max(nnz, 1), dtype=np.int32)   # never NULL, even when empty
+    val = np.empty(max(nnz, 1), dtype=np.float64)
     av, bv = _f64(A.val), _f64(B.val)
     st = lib().oracle_numeric(A.nrows, B.ncols, _p(A.rowptr), _p(A.col), _p(av), _p(B.rowptr),
                               _p(B.col), _p(bv), _p(rp), _p(col), _p(val), nthreads)
     if st:
         raise RuntimeError(f"oracle_numeric failed: {st}")
-    return rp, col, val
+    return rp, col[:nnz], val[:nnz]
 
 
 def spgemm_rows(A, B, r0, r1, nthreads=0):
@@ -105,15 +105,15 @@ def spgemm_rows(A, B, r0, r1, nthreads=0):
                                      _p(B.col), _p(rp), nthreads)
     if nnz < 0:
         raise RuntimeError(f"oracle_symbolic_rows failed: {nnz}")
-    col = np.empty(int(nnz), dtype=np.int32)
-    val = np.empty(int(nnz), dtype=np.float64)
+    col = np.empty(max(int(nnz), 1), dtype=np.int32)
+    val = np.empty(max(int(nnz), 1), dtype=np.float64)
     av, bv = _f64(A.val), _f64(B.val)
     st = lib().oracle_numeric_rows(r0, r1, B.ncols, _p(A.rowptr), _p(A.col), _p(av),
                                    _p(B.rowptr), _p(B.col), _p(bv), _p(rp), _p(col), _p(val),
                                    nthreads)
     if st:
         raise RuntimeError(f"oracle_numeric_rows failed: {st}")
-    return rp, col, val
+    return rp, col[:int(nnz)], val[:int(nnz)]
 
 
 def absbound(A, B, rp, col, nthreads=0):

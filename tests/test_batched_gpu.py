@@ -58,11 +58,15 @@ def test_batched_equals_single_calls(cuda):
     dA = [a.to_device() for a, _ in pairs]
     dB = [b.to_device() for _, b in pairs]
     Cs = nb.spgemm_batched(dA, dB)
-    for got, a, b in zip(Cs, dA, dB):
-        one = nb.spgemm(a, b).to_host()
+    for got, a, b, (A, B) in zip(Cs, dA, dB, pairs):
+        one, st = nb.spgemm(a, b, return_stats=True)
+        one = one.to_host()
         h = got.to_host()
         assert_same_structure(h.rowptr, h.col, one.rowptr, one.col)
-        assert_bitwise(h.val, one.val)
+        if sum(st["num_bins"][6:]) == 0:
+            assert_bitwise(h.val, one.val)
+        else:  # rows on the block path add atomically, in any order
+            assert_close(h.val, one.val, oracle.absbound(A, B, one.rowptr, one.col))
 
 
 def test_batched_fp32c(cuda):
