@@ -34,9 +34,12 @@ constexpr int kNumGroupBins = 6;
 constexpr int kSymLong = kSymBins - 1;
 constexpr int kNumLong = kNumBins - 1;
 
-// Inclusive upper limits of each bin (the last bin is unbounded).
+// Inclusive upper limits of each bin (the last bin is unbounded). A symbolic
+// bin of table size T = 32 << b takes rows with ub <= 0.75 T, so a row whose
+// distinct columns reach its bound still leaves a quarter of the table free
+// (linear probing slows sharply past that load).
 __host__ __device__ constexpr int sym_limit(int b) {
-  return b < kSymLong ? (32 << b) : 0x7fffffff;  // 32,64,...,32768
+  return b < kSymLong ? (24 << b) : 0x7fffffff;  // 24,48,...,24576
 }
 __host__ __device__ constexpr int num_limit(int b) {
   return b < kNumLong ? (16 << b) : 0x7fffffff;  // 16,32,...,4096

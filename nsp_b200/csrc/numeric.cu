@@ -20,8 +20,14 @@
 #include "common.cuh"
 #include "internal.h"
 #include "launch_util.h"
+#include "spgemm_host.h"
+
+#include <algorithm>
 
 namespace nspb {
+
+// Device memory the long-row kernel may use for its per-CTA accumulators.
+constexpr long long kDenseBudget = 4LL << 30;
 
 // ---- row groups -------------------------------------------------------------------
 template <int G, int LOG2T>
@@ -31,7 +37,8 @@ struct NumGroupCfg {
   static constexpr int NB = T / 2;      // sort buckets
   // per-group stride, rounded to 16 bytes so every group's fp64 arrays stay
   // 8-byte aligned
-  static constexpr int BYTES = (T * 12 + H * 12 + NB * 4 + 15) & ~15;
+  // the table's upper half doubles as the bucket buffer of the sort
+  static constexpr int BYTES = (T * 12 + NB * 4 + 15) & ~15;
   static constexpr int kBySmem = (56 * 1024) / BYTES > 0 ? (56 * 1024) / BYTES : 1;
   static constexpr int GPC = kBySmem < 256 / G ? kBySmem : 256 / G;
   static constexpr int THREADS = GPC * G;
@@ -64,10 +71,8 @@ __global__ void __launch_bounds__(256)
   const int lane = tile.thread_rank();
   unsigned char *gb = smem_num + (size_t)g * C::BYTES;
   double *vals = reinterpret_cast<double *>(gb);
-  double *bvals = vals + C::T;
-  int *keys = reinterpret_cast<int *>(bvals + C::H);
-  int *bkeys = keys + C::T;
-  int *cnt = bkeys + C::H;
+  int *keys = reinterpret_cast<int *>(vals + C::T);
+  int *cnt = keys + C::T;
 
   int my_max_deg = 0, my_redo = 0;  // compensated mode, flushed once per group
   for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
@@ -136,44 +141,66 @@ __global__ void __launch_bounds__(256)
     const int n = crpt[row + 1] - c0;
     mn = cg::reduce(tile, mn, cg::less<int>());
     mx = cg::reduce(tile, mx, cg::greater<int>());
-    // -- bucket sort: histogram, scan, scatter, rank within bucket
+    // -- bucket sort. (1) compact the occupied slots to the front of the
+    // table in slot order while counting buckets; (2) scan the counts;
+    // (3) scatter into the table's free upper half [H, H+n); (4) rank inside
+    // each bucket, writing the sorted row back to [0, n).
     for (int b = lane; b < C::NB; b += G) cnt[b] = 0;
     tile.sync();
     const float scale = n > 0 ? (float)C::NB / (float)((long long)mx - mn + 1) : 0.f;
-    for (int s = lane; s < C::T; s += G) {
-      const int key = keys[s];
-      if (key >= 0) atomicAdd(&cnt[bucket_of(key, mn, scale, C::NB)], 1);
+    int occ_total = 0;
+    for (int base = 0; base < C::T; base += G) {
+      const int key = keys[base + lane];
+      const double v = vals[base + lane];
+      const unsigned ball = tile.ballot(key >= 0);
+      tile.sync();  // every lane has read its slot before any slot is rewritten
+      if (key >= 0) {
+        const int pos = occ_total + __popc(ball & ((1u << lane) - 1u));
+        keys[pos] = key;
+        vals[pos] = v;
+        atomicAdd(&cnt[bucket_of(key, mn, scale, C::NB)], 1);
+      }
+      occ_total += __popc(ball);
+      tile.sync();
+    }
+    if constexpr (C::PER <= 8) {  // each lane scans a run of PER counters in registers
+      int local[C::PER];
+      int sum = 0;
+#pragma unroll
+      for (int q = 0; q < C::PER; ++q) {
+        const int idx = lane * C::PER + q;
+        local[q] = idx < C::NB ? cnt[idx] : 0;
+        sum += local[q];
+      }
+      int ex = cg::exclusive_scan(tile, sum, cg::plus<int>());
+#pragma unroll
+      for (int q = 0; q < C::PER; ++q) {
+        const int idx = lane * C::PER + q;
+        if (idx < C::NB) cnt[idx] = ex;
+        ex += local[q];
+      }
+    } else {  // rounds of G consecutive counters
+      int run = 0;
+      for (int base = 0; base < C::NB; base += G) {
+        const int v = cnt[base + lane];
+        const int incl = cg::inclusive_scan(tile, v, cg::plus<int>());
+        cnt[base + lane] = run + incl - v;
+        run += tile.shfl(incl, G - 1);
+      }
     }
     tile.sync();
-    int local[C::PER];
-    int sum = 0;
-#pragma unroll
-    for (int q = 0; q < C::PER; ++q) {
-      const int idx = lane * C::PER + q;
-      local[q] = idx < C::NB ? cnt[idx] : 0;
-      sum += local[q];
-    }
-    int ex = cg::exclusive_scan(tile, sum, cg::plus<int>());
-    const int tot = tile.shfl(ex + sum, G - 1);
-#pragma unroll
-    for (int q = 0; q < C::PER; ++q) {
-      const int idx = lane * C::PER + q;
-      if (idx < C::NB) cnt[idx] = ex;
-      ex += local[q];
-    }
-    tile.sync();
-    if (tot != n || n > C::H) {  // symbolic/numeric disagreement: skip the row
+    if (occ_total != n || n > C::H) {  // symbolic/numeric disagreement: skip the row
       if (lane == 0) atomicOr(err, ERR_COUNT);
       tile.sync();
       continue;
     }
-    for (int s = lane; s < C::T; s += G) {
-      const int key = keys[s];
-      if (key >= 0) {
-        const int pos = atomicAdd(&cnt[bucket_of(key, mn, scale, C::NB)], 1);
-        bkeys[pos] = key;
-        bvals[pos] = vals[s];
-      }
+    int *bkeys = keys + C::H;
+    double *bvals = vals + C::H;
+    for (int q = lane; q < n; q += G) {
+      const int key = keys[q];
+      const int pos = atomicAdd(&cnt[bucket_of(key, mn, scale, C::NB)], 1);
+      bkeys[pos] = key;
+      bvals[pos] = vals[q];
     }
     tile.sync();
     for (int q = lane; q < n; q += G) {
@@ -467,6 +494,106 @@ __global__ void __launch_bounds__(kNumLongThreads)
   if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
 }
 
+// ---- longest rows: dense fp64 accumulator in global memory ---------------------
+// Each CTA owns an ncols-long fp64 accumulator in device memory (zero between
+// rows) and a shared-memory bitmap over a 2^20-column window. Products are
+// added with global fp64 atomics (one pass over the row's products for
+// ncols <= 2^20), then the set bits are emitted in column order, each value
+// read and its slot zeroed. acc is read and written with .cg accesses (L2
+// only) so no stale L1 line is seen after another thread's atomic.
+constexpr int kDenseBits = 1 << 20;
+constexpr int kDenseWords = kDenseBits / 32;
+
+template <typename VT>
+__global__ void __launch_bounds__(kNumLongThreads)
+    k_num_long_dense(const int *__restrict__ arpt, const int *__restrict__ acol,
+                     const VT *__restrict__ aval, const int *__restrict__ brpt,
+                     const int *__restrict__ bcol, const VT *__restrict__ bval, int ncols,
+                     const int *__restrict__ crpt, int *__restrict__ ccol,
+                     double *__restrict__ cval, const int *__restrict__ rows, int count,
+                     double *__restrict__ acc_all, int *__restrict__ err,
+                     int *__restrict__ redo) {
+  extern __shared__ __align__(16) unsigned bm_dense[];
+  __shared__ int red[kNumLongThreads / 32];
+  double *acc = acc_all + (size_t)blockIdx.x * (size_t)ncols;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int W = kNumLongThreads / 32;
+  int rows_done = 0;
+  for (int r = blockIdx.x; r < count; r += gridDim.x) {
+    const int row = rows ? rows[r] : r;
+    const int a0 = arpt[row], a1 = arpt[row + 1];
+    int off = crpt[row];
+    const int row_end = crpt[row + 1];
+    for (int w0 = 0; w0 < ncols; w0 += kDenseBits) {
+      const int wn = min(kDenseBits, ncols - w0);
+      const int words = (wn + 31) >> 5;
+      for (int q = threadIdx.x; q < words; q += kNumLongThreads) bm_dense[q] = 0u;
+      __syncthreads();
+      for (int j = a0 + warp; j < a1; j += W) {
+        const int k = ld_stream(acol + j);
+        const double a = ldv_stream(aval + j);
+        const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
+        for (int e = s0 + lane; e < s1; e += 32) {
+          const int c = __ldg(bcol + e);
+          const unsigned d = (unsigned)(c - w0);
+          if (d < (unsigned)wn) {
+            atomicAdd(acc + c, __dmul_rn(a, ldv(bval + e)));
+            const unsigned bit = 1u << (d & 31u);
+            if (!(bm_dense[d >> 5] & bit)) atomicOr(bm_dense + (d >> 5), bit);
+          }
+        }
+      }
+      __threadfence_block();
+      __syncthreads();
+      // emit in column order, one round of kNumLongThreads words at a time
+      for (int base = 0; base < words; base += kNumLongThreads) {
+        const int w = base + threadIdx.x;
+        const unsigned m0 = w < words ? bm_dense[w] : 0u;
+        const int pc = __popc(m0);
+        int incl = pc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        if (lane == 31) red[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+          int v = red[lane];
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+          }
+          red[lane] = v;
+        }
+        __syncthreads();
+        const int rtot = red[W - 1];
+        int pos = off + (warp ? red[warp - 1] : 0) + incl - pc;
+        unsigned m = m0;
+        if (pos + pc > row_end) {  // more entries than the symbolic count: write nothing
+          if (pc) atomicOr(err, ERR_COUNT);
+          m = 0u;
+        }
+        while (m) {
+          const int b = __ffs(m) - 1;
+          m &= m - 1u;
+          const int c = w0 + w * 32 + b;
+          ccol[pos] = c;
+          cval[pos] = __ldcg(acc + c);
+          __stcg(acc + c, 0.0);
+          ++pos;
+        }
+        off += rtot;
+        __syncthreads();
+      }
+    }
+    if (threadIdx.x == 0 && off != row_end) atomicOr(err, ERR_COUNT);
+    ++rows_done;
+  }
+  if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
+}
+
 // ---- dispatch ------------------------------------------------------------------------
 template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>
 static cudaError_t run_num_group(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
@@ -540,9 +667,31 @@ static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, 
     case kNumGroupBins + 2:
       return run_num_block<13, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
     default: {
+      // dense accumulator per CTA when its footprint fits kDenseBudget,
+      // else shared-memory column windows
+      const int dsmem = kDenseWords * 4;
+      const void *fd = (const void *)k_num_long_dense<VT>;
+      int grid = persistent_grid(fd, kNumLongThreads, dsmem, count, 1);
+      const long long per_cta = 8LL * (B.ncols > 0 ? B.ncols : 1);
+      const long long fit = kDenseBudget / per_cta;
+      if (grid > 0 && fit >= 1) {
+        grid = (int)std::min<long long>(grid, fit);
+        double *acc = nullptr;
+        if (scratch_alloc(reinterpret_cast<void **>(&acc), (size_t)per_cta * grid, s) == NSPB_OK) {
+          cudaError_t e = cudaMemsetAsync(acc, 0, (size_t)per_cta * grid, s);
+          if (e == cudaSuccess) {
+            k_num_long_dense<VT><<<grid, kNumLongThreads, dsmem, s>>>(
+                A.rpt, A.col, av, B.rpt, B.col, bv, B.ncols, crpt, ccol, cval, rows, count, acc,
+                err, redo);
+            e = cudaGetLastError();
+          }
+          scratch_free(acc, s);
+          return e;
+        }
+      }
       const int smem = kWin * 8 + kWinWords * 4;
       const void *f = (const void *)k_num_long<VT>;
-      const int grid = persistent_grid(f, kNumLongThreads, smem, count, 1);
+      grid = persistent_grid(f, kNumLongThreads, smem, count, 1);
       if (grid <= 0) return cudaErrorInvalidConfiguration;
       k_num_long<VT><<<grid, kNumLongThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv,
                                                          B.ncols, b_sorted, crpt, ccol, cval,
