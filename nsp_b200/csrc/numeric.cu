@@ -29,6 +29,23 @@ namespace nspb {
 // Device memory the long-row kernel may use for its per-CTA accumulators.
 constexpr long long kDenseBudget = 4LL << 30;
 
+// Rank of `key` among the bucket-ordered keys bk[0..n): its bucket spans
+// [st, en). Reads 4 keys per shared-memory load from st rounded down to a
+// multiple of 4: keys before st lie in earlier buckets, so they are smaller
+// and are counted (the base is u0, not st); keys from en on lie in later
+// buckets and are larger, so they are not; indices >= n are masked out.
+// bk must be 16-byte aligned.
+__device__ __forceinline__ int rank_in_bucket(const int *bk, int st, int en, int n, int key) {
+  const int u0 = st & ~3;
+  int rank = u0;
+  for (int u = u0; u < en; u += 4) {
+    const int4 v = *reinterpret_cast<const int4 *>(bk + u);
+    rank += (v.x < key) + ((u + 1 < n) & (v.y < key)) + ((u + 2 < n) & (v.z < key)) +
+            ((u + 3 < n) & (v.w < key));
+  }
+  return rank;
+}
+
 // ---- row groups -------------------------------------------------------------------
 template <int G, int LOG2T>
 struct NumGroupCfg {
@@ -207,8 +224,7 @@ __global__ void __launch_bounds__(256)
       const int key = bkeys[q];
       const int b = bucket_of(key, mn, scale, C::NB);
       const int st = b ? cnt[b - 1] : 0, en = cnt[b];
-      int rank = st;
-      for (int u = st; u < en; ++u) rank += bkeys[u] < key;
+      const int rank = rank_in_bucket(bkeys, st, en, n, key);
       keys[rank] = key;
       vals[rank] = bvals[q];
     }
@@ -356,8 +372,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
       const int key = bkeys[q];
       const int b = bucket_of(key, mn, scale, NB);
       const int st = b ? cnt[b - 1] : 0, en = cnt[b];
-      int rank = st;
-      for (int u = st; u < en; ++u) rank += bkeys[u] < key;
+      const int rank = rank_in_bucket(bkeys, st, en, n, key);
       keys[rank] = key;
       vals[rank] = bvals[q];
     }
