@@ -56,6 +56,8 @@ def parse():
                    choices=["stencil27", "amg_batch", "fp32c", "powerlaw"],
                    help="stencil27: the headline line; amg_batch: batched vs one call per "
                         "product; fp32c: compensated fp32 vs fp64 on the 27-point stencil")
+    p.add_argument("--pl-rows", type=int, default=1_000_000,
+                   help="power-law matrix order (default 1M; smaller for profiler captures)")
     p.add_argument("--batch-count", type=int, default=256)
     p.add_argument("--batch-nmax", type=int, default=100_000)
     return p.parse_args()
@@ -138,7 +140,7 @@ def run_powerlaw(args):
     16, max 50k): every bin, including the long-row kernels."""
     import torch
     import nsp_b200 as nb
-    P = nb.gen.powerlaw(1_000_000, alpha=2.1, mean_deg=16.0, max_deg=50_000, seed=SEED)
+    P = nb.gen.powerlaw(args.pl_rows, alpha=2.1, mean_deg=16.0, max_deg=50_000, seed=SEED)
     dP = P.to_device()
     C0, st0 = nb.spgemm(dP, dP, return_stats=True)
     nnz = st0["nnz"]
@@ -154,11 +156,12 @@ def run_powerlaw(args):
     ms = _timed(step, args.steps, max(args.warmup, 1))
     _, st = nb.spgemm(dP, dP, out=out, return_stats=True)
     print(json.dumps({
-        "metric": "SpGEMM GFLOP/s, C=A*A, power-law n=1M (alpha 2.1, mean 16, max 50k), fp64",
+        "metric": f"SpGEMM GFLOP/s, C=A*A, power-law n={args.pl_rows} (alpha 2.1, mean 16, "
+                  "max 50k), fp64",
         "value": 2 * st0["intprod"] / ms / 1e6, "unit": "GFLOP/s", "n_gpus": 1,
         "steps": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": ms,
         "higher_is_better": True, "dtype": "f64", "data": f"synthetic (seed {SEED})",
-        "config": {"workload": "powerlaw_1M_AxA_fp64", "nnz_A": P.nnz,
+        "config": {"workload": f"powerlaw_{args.pl_rows}_AxA_fp64", "nnz_A": P.nnz,
                    "xmin": nb.gen.powerlaw_xmin(), "intprod": st0["intprod"], "nnz_C": nnz,
                    "sym_bins": st["sym_bins"], "num_bins": st["num_bins"]},
         "effective_gbs": alg_bytes(P, P, nnz) / (ms * 1e-3) / 1e9}), flush=True)

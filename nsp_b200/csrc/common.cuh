@@ -175,6 +175,166 @@ __device__ __forceinline__ double ldv_stream(const float *p) {
   return (double)v;
 }
 
+// Shared state of row_products: a queue of one round's A entries {B row
+// start, B row end, A value as two ints} and two sets of counters {medium
+// entries, long entries, medium cursor}, used in alternate rounds so that one
+// set is cleared while the other is in use. Counters start at zero.
+template <int THREADS>
+struct RowQueue {
+  int4 q[THREADS];
+  int ctr[2][3];
+};
+
+template <int THREADS>
+__device__ __forceinline__ void row_queue_init(RowQueue<THREADS> &rq) {
+  if (threadIdx.x < 6) (&rq.ctr[0][0])[threadIdx.x] = 0;
+}
+
+// Every product of one A row, spread evenly over a block of THREADS threads
+// whatever the lengths of the B rows it touches (power-law matrices mix rows
+// of one entry with hub rows of 10^4 and more). The A row is taken in rounds
+// of THREADS entries, one per thread:
+//   - a B row of at most 32 entries (4 when the round holds fewer than
+//     THREADS/4 entries) is walked by its thread: up to THREADS independent
+//     gather chains in flight;
+//   - a longer B row goes to a queue; warps take queued rows one at a time
+//     from a shared cursor, lanes over the row's entries;
+//   - a B row of THREADS entries or more is walked by the whole block, thread
+//     t taking the products whose index in the round's concatenation of such
+//     rows is t mod THREADS.
+// f(e, a) gets the B entry index and the A value (0 when aval is null). Every
+// thread of the block must call this with the same (a0, a1) after a block
+// barrier, and a block barrier must separate two calls.
+template <int THREADS, typename VT, typename F>
+__device__ __forceinline__ void row_products(const int *__restrict__ acol,
+                                             const VT *__restrict__ aval,
+                                             const int *__restrict__ brpt, int a0, int a1,
+                                             RowQueue<THREADS> &rq, F &&f) {
+  static_assert((THREADS & (THREADS - 1)) == 0, "THREADS must be a power of two");
+  const int lane = threadIdx.x & 31;
+  int par = 0;
+  for (int jr = a0; jr < a1; jr += THREADS, par ^= 1) {  // uniform across the block
+    const int small_max = min(THREADS, a1 - jr) * 4 >= THREADS ? 32 : 4;
+    const int j = jr + (int)threadIdx.x;
+    if (j < a1) {
+      const int k = ld_stream(acol + j);
+      const double a = aval ? ldv_stream(aval + j) : 0.0;
+      const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
+      if (s1 - s0 <= small_max) {
+        for (int e = s0; e < s1; ++e) f(e, a);
+      } else {
+        const int big = (s1 - s0 >= THREADS) ? 1 : 0;
+        const int slot = atomicAdd(&rq.ctr[par][big], 1);
+        rq.q[big ? THREADS - 1 - slot : slot] =
+            make_int4(s0, s1, __double2loint(a), __double2hiint(a));
+      }
+    }
+    __syncthreads();
+    // the other counter set was last read before the previous round's closing
+    // barrier and is next written after this round's
+    if (threadIdx.x == 0) rq.ctr[par ^ 1][0] = rq.ctr[par ^ 1][1] = rq.ctr[par ^ 1][2] = 0;
+    const int nm = rq.ctr[par][0], nb = rq.ctr[par][1];
+    for (;;) {
+      int i = 0;
+      if (lane == 0) i = atomicAdd(&rq.ctr[par][2], 1);
+      i = __shfl_sync(0xffffffffu, i, 0);
+      if (i >= nm) break;
+      const int4 v = rq.q[i];
+      const double a = __hiloint2double(v.w, v.z);
+      for (int e = v.x + lane; e < v.y; e += 32) f(e, a);
+    }
+    unsigned pos = 0;  // products of the long rows before row i, mod 2^32
+    for (int i = 0; i < nb; ++i) {
+      const int4 v = rq.q[THREADS - 1 - i];
+      const double a = __hiloint2double(v.w, v.z);
+      const int first = (int)((threadIdx.x - pos) & (unsigned)(THREADS - 1));
+      for (int e = v.x + first; e < v.y; e += THREADS) f(e, a);
+      pos += (unsigned)(v.y - v.x);
+    }
+    __syncthreads();
+  }
+  // counters of the last round (the other set was cleared during it); the
+  // caller's barrier before the next call orders this
+  if (a1 > a0 && threadIdx.x == 0)
+    rq.ctr[par ^ 1][0] = rq.ctr[par ^ 1][1] = rq.ctr[par ^ 1][2] = 0;
+}
+
+// Intermediate products of one A row and the range of columns they can
+// reach: [lo, hi] from the first and last entries of the B rows it touches
+// when B's rows are sorted, else [0, ncols). Empty rows give lo > hi.
+struct RowSpan {
+  long long ip;
+  int lo, hi;
+};
+
+template <int THREADS>
+struct SpanScratch {
+  long long ip[THREADS / 32];
+  int lo[THREADS / 32], hi[THREADS / 32];
+};
+
+// Block-wide; every thread gets the row's span. Ends with a block barrier
+// and reads sc after it, so a block barrier must come before the next call.
+template <int THREADS>
+__device__ __forceinline__ RowSpan row_span(const int *__restrict__ acol,
+                                            const int *__restrict__ brpt,
+                                            const int *__restrict__ bcol, int a0, int a1,
+                                            bool b_sorted, int ncols, SpanScratch<THREADS> &sc) {
+  constexpr int W = THREADS / 32;
+  long long ip = 0;
+  int lo = 0x7fffffff, hi = -1;
+  for (int j = a0 + (int)threadIdx.x; j < a1; j += THREADS) {
+    const int k = __ldg(acol + j);
+    const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
+    if (s1 > s0) {
+      ip += s1 - s0;
+      if (b_sorted) {
+        lo = min(lo, __ldg(bcol + s0));
+        hi = max(hi, __ldg(bcol + s1 - 1));
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ip += __shfl_xor_sync(0xffffffffu, ip, o);
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    sc.ip[warp] = ip;
+    sc.lo[warp] = lo;
+    sc.hi[warp] = hi;
+  }
+  __syncthreads();
+  RowSpan r{0, 0x7fffffff, -1};
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    r.ip += sc.ip[w];
+    r.lo = min(r.lo, sc.lo[w]);
+    r.hi = max(r.hi, sc.hi[w]);
+  }
+  if (!b_sorted && r.ip > 0) {
+    r.lo = 0;
+    r.hi = ncols - 1;
+  }
+  // columns outside [0, ncols) fall outside every window and are dropped
+  r.lo = max(r.lo, 0);
+  r.hi = min(r.hi, ncols - 1);
+  return r;
+}
+
+// Next row index of a block-per-row kernel from a launch-wide ticket counter
+// (zero at launch): rows go to blocks as they free up, so a block that drew a
+// heavy row draws no more meanwhile. Returns count when none is left.
+__device__ __forceinline__ int next_row(int *ticket, int count, int *s_slot) {
+  __syncthreads();  // every thread has read the previous slot value
+  if (threadIdx.x == 0) *s_slot = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int r = *s_slot;
+  return r < count ? r : count;
+}
+
 // Padded index of a bucket counter: one spare slot per 32 counters, so a
 // lane that owns a run of consecutive counters hits its own bank.
 __device__ __forceinline__ int cpad(int b) { return b + (b >> 5); }

@@ -57,17 +57,21 @@ cudaError_t launch_num_hist(const int *crpt, int n, int *num_counts,
                             cudaStream_t s);
 
 // ---- symbolic.cu ----------------------------------------------------------------
-cudaError_t launch_symbolic_bin(int bin, int lanes, const CsrDev &A,
+// ticket: a zeroed counter for this launch (block-per-row kernels hand out
+// rows with it). b_sorted: B rows strictly increasing (a row's column span
+// then comes from the ends of the B rows it touches).
+cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const CsrDev &A,
                                 const CsrDev &B, const int *rows, int count,
-                                int *row_nz, int *err, cudaStream_t s);
+                                int *row_nz, int *err, int *ticket, cudaStream_t s);
 
 // ---- numeric.cu -----------------------------------------------------------------
 // owned: B rows hold no duplicate columns (deterministic plain accumulation).
-// b_sorted: B rows strictly increasing (long rows use binary search).
+// b_sorted: B rows strictly increasing (long rows take their column span
+// from the ends of the B rows they touch).
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
                                const CsrDev &A, const CsrDev &B,
                                const int *crpt, int *ccol, double *cval,
-                               const int *rows, int count, int *err,
+                               const int *rows, int count, int *err, int *ticket,
                                cudaStream_t s);
 
 // Compensated numeric step (fp32 inputs): rows with at most nmax A entries
@@ -79,6 +83,6 @@ cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorte
                                     const CsrDev &A, const CsrDev &B, const int *crpt,
                                     int *ccol, double *cval, const int *rows, int count,
                                     int nmax, int *redo, int *max_deg, int *err,
-                                    cudaStream_t s);
+                                    int *ticket, cudaStream_t s);
 
 }  // namespace nspb

@@ -12,8 +12,34 @@
 
 namespace nspb {
 
-// Resident CTAs per SM for `func` at (threads, smem); sets the opt-in
-// dynamic shared memory limit first when smem > 48 KB. Returns 0 on error.
+// Raises the dynamic shared memory limit of `func` to what the device allows
+// beside its static shared memory, once per (device, kernel): launches of one
+// kernel may then use any size up to that (a kernel whose static and dynamic
+// parts add up past 48 KB needs the opt-in even when the dynamic part alone
+// does not). Returns false on error.
+inline bool allow_smem(const void *func) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, bool> done;
+  const int dev = dev_info().device;
+  const auto key = std::make_pair(dev, func);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find(key);
+  if (it != done.end()) return it->second;
+  cudaFuncAttributes fa;
+  bool ok = cudaFuncGetAttributes(&fa, func) == cudaSuccess;
+  if (ok) {
+    const int dyn = dev_info().smem_optin - (int)fa.sharedSizeBytes;
+    ok = dyn > 0 &&
+         cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ==
+             cudaSuccess;
+  }
+  if (!ok) cudaGetLastError();
+  done[key] = ok;
+  return ok;
+}
+
+// Resident CTAs per SM for `func` at (threads, smem), after raising its
+// dynamic shared memory limit. Returns 0 on error.
 inline int resident_ctas(const void *func, int threads, int smem) {
   static std::mutex mu;
   static std::map<std::tuple<int, const void *, int, int>, int> cache;
@@ -24,10 +50,7 @@ inline int resident_ctas(const void *func, int threads, int smem) {
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
   }
-  if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-      return 0;
-  }
+  if (!allow_smem(func)) return 0;
   int blocks = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, func, threads, (size_t)smem) != cudaSuccess)
     return 0;

@@ -7,9 +7,11 @@
 //   ..._each_tb_outsort + nsp_calc_val_sort_rows  :1632-1714,
 //                                          nsp_calc_val_sort_rows.cu:24-527
 //   ..._chunk_dynamic / nsp_calc_C_dense / ..._chunk_B_dense :1725-2151
-// The reference sorts each row by an O(nnz^2) rank count. Here each row is
-// sorted by a monotone bucket scatter over [min col, max col] followed by a
-// rank count inside each bucket, in shared memory, and written coalesced.
+// The reference sorts each row by an O(nnz^2) rank count. Here each row of up
+// to 4096 entries is sorted by a monotone bucket scatter over [min col, max
+// col] followed by a rank count inside each bucket, in shared memory, and
+// written coalesced; longer rows need no sort at all: a bitmap of their
+// columns gives each column its output position (k_num_rank).
 //
 // Row groups of G lanes walk the A row in order and cover one B row per step
 // (B rows hold no repeated column when `owned`), so each slot of the hash
@@ -25,9 +27,6 @@
 #include <algorithm>
 
 namespace nspb {
-
-// Device memory the long-row kernel may use for its per-CTA accumulators.
-constexpr long long kDenseBudget = 4LL << 30;
 
 // Rank of `key` among the bucket-ordered keys bk[0..n): its bucket spans
 // [st, en). Reads 4 keys per shared-memory load from st rounded down to a
@@ -279,7 +278,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
                 const int *__restrict__ bcol, const VT *__restrict__ bval,
                 const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
-                int *__restrict__ err, int *__restrict__ redo) {
+                int *__restrict__ err, int *__restrict__ redo, int *__restrict__ ticket) {
   constexpr int T = 1 << LOG2T, H = T / 2, NB = T / 2;
   constexpr int PER = NB / kNumBlockThreads;
   extern __shared__ __align__(16) unsigned char smem_num[];
@@ -289,11 +288,12 @@ __global__ void __launch_bounds__(kNumBlockThreads)
   int *bkeys = keys + T;
   int *cnt = bkeys + H;
   __shared__ int red[kNumBlockThreads / 32];
-  __shared__ int s_mn, s_mx;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int W = kNumBlockThreads / 32;
+  __shared__ int s_mn, s_mx, s_slot;
+  __shared__ RowQueue<kNumBlockThreads> rq;
+  row_queue_init(rq);
+  const int lane = threadIdx.x & 31;
   int rows_done = 0;
-  for (int r = blockIdx.x; r < count; r += gridDim.x) {
+  for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
     for (int s = threadIdx.x; s < T; s += kNumBlockThreads) {
       keys[s] = kEmpty;
@@ -307,17 +307,12 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     __syncthreads();
     const int a0 = arpt[row], a1 = arpt[row + 1];
     int mn = 0x7fffffff, mx = -1;
-    for (int j = a0 + warp; j < a1; j += W) {
-      const int k = ld_stream(acol + j);
-      const double a = ldv_stream(aval + j);
-      const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
-      for (int e = s0 + lane; e < s1; e += 32) {
-        const int key = __ldg(bcol + e);
-        num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, ldv(bval + e)), err);
-        mn = min(mn, key);
-        mx = max(mx, key);
-      }
-    }
+    row_products<kNumBlockThreads>(acol, aval, brpt, a0, a1, rq, [&](int e, double a) {
+      const int key = __ldg(bcol + e);
+      num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, ldv(bval + e)), err);
+      mn = min(mn, key);
+      mx = max(mx, key);
+    });
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
@@ -386,227 +381,177 @@ __global__ void __launch_bounds__(kNumBlockThreads)
   if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
 }
 
-// ---- longest rows: dense column windows in shared memory ----------------------------
-constexpr int kNumLongThreads = 1024;
-constexpr int kWin = 16384;            // columns per window: 128 KB of fp64
-constexpr int kWinWords = kWin / 32;   // occupancy bitmap
+// ---- rows of more than 4096 entries: column ranks from a row bitmap -----------
+// A first pass over the row's products sets its distinct columns as bits of a
+// shared-memory bitmap over the row's column span [lo, hi] (see row_span). A
+// prefix count of the bitmap then gives every column its rank, which is its
+// position in the sorted output row: the columns are written in order with no
+// sort, and a second pass adds each product straight into its output slot,
+// in shared memory when the row has at most kRankVals entries, else with fp64
+// atomics into the row's part of C.val (which stays in L2 while the row is
+// built: 8 bytes per entry). A span wider than 2^20 columns is covered in
+// windows of 2^20, each with its own two passes.
+//
+// Thread t owns the 64-bit words [t*per, (t+1)*per) of a window's bitmap, so
+// warp w owns 32*per words; the rank of column c is base[warp of c] +
+// pre[c/64] + the bits below c in its word, pre[] being the 16-bit count
+// inside the warp's words (at most 511*64 bits precede a word there).
+constexpr int kRankThreads = 1024;
+constexpr int kRankVals = 6144;          // 48 KB of fp64 accumulators
+constexpr int kRankMaxCols = 1 << 20;    // bitmap of 2^14 64-bit words, 128 KB
+#ifndef NSPB_RANK_FROM_BIN
+#define NSPB_RANK_FROM_BIN kNumLong
+#endif
+constexpr int kRankFromBin = NSPB_RANK_FROM_BIN;  // first numeric bin sent here
 
-__device__ __forceinline__ int lower_bound_col(const int *__restrict__ col, int lo, int hi, int c) {
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(col + mid) < c) lo = mid + 1; else hi = mid;
-  }
-  return lo;
+// log2 of the 64-bit words per thread for a window of `cols` columns
+__host__ __device__ inline int rank_per_log2(int cols) {
+  int pl = 0;
+  while (pl < 4 && (kRankThreads << (pl + 6)) < cols) ++pl;
+  return pl;
+}
+__host__ __device__ constexpr int rank_smem(int per_log2) {
+  return (kRankThreads << per_log2) * 10 + kRankVals * 8;
 }
 
 template <typename VT>
-__global__ void __launch_bounds__(kNumLongThreads)
-    k_num_long(const int *__restrict__ arpt, const int *__restrict__ acol,
+__global__ void __launch_bounds__(kRankThreads)
+    k_num_rank(const int *__restrict__ arpt, const int *__restrict__ acol,
                const VT *__restrict__ aval, const int *__restrict__ brpt,
-               const int *__restrict__ bcol, const VT *__restrict__ bval,
-               int ncols, bool sorted, const int *__restrict__ crpt,
+               const int *__restrict__ bcol, const VT *__restrict__ bval, int ncols,
+               int b_sorted, int pl_max, const int *__restrict__ crpt,
                int *__restrict__ ccol, double *__restrict__ cval,
                const int *__restrict__ rows, int count, int *__restrict__ err,
-               int *__restrict__ redo) {
-  extern __shared__ __align__(16) unsigned char smem_num[];
-  double *dense = reinterpret_cast<double *>(smem_num);
-  unsigned *bm = reinterpret_cast<unsigned *>(dense + kWin);
-  __shared__ int red[kNumLongThreads / 32];
+               int *__restrict__ redo, int *__restrict__ ticket) {
+  extern __shared__ __align__(16) unsigned long long bm64[];
+  const int max_words = kRankThreads << pl_max;
+  unsigned *bm32 = reinterpret_cast<unsigned *>(bm64);
+  unsigned short *pre = reinterpret_cast<unsigned short *>(bm64 + max_words);
+  double *vals = reinterpret_cast<double *>(pre + max_words);  // max_words*2: multiple of 8
+  __shared__ int base[kRankThreads / 32];
+  __shared__ int s_total, s_slot;
+  __shared__ RowQueue<kRankThreads> rq;
+  __shared__ SpanScratch<kRankThreads> sc;
+  row_queue_init(rq);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int W = kNumLongThreads / 32;
   int rows_done = 0;
-  for (int r = blockIdx.x; r < count; r += gridDim.x) {
+  for (int q = threadIdx.x; q < max_words; q += kRankThreads) bm64[q] = 0ull;
+  for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
     const int a0 = arpt[row], a1 = arpt[row + 1];
-    const bool per_thread = (a1 - a0) >= kNumLongThreads;
-    int off = crpt[row];
     const int row_end = crpt[row + 1];
-    for (int w0 = 0; w0 < ncols; w0 += kWin) {
-      const int w1 = w0 + kWin;
-      for (int s = threadIdx.x; s < kWin; s += kNumLongThreads) dense[s] = 0.0;
-      for (int s = threadIdx.x; s < kWinWords; s += kNumLongThreads) bm[s] = 0u;
-      __syncthreads();
-      if (per_thread) {  // one A entry per thread
-        for (int j = a0 + threadIdx.x; j < a1; j += kNumLongThreads) {
-          const int k = ld_stream(acol + j);
-          const double a = ldv_stream(aval + j);
-          const int s1 = __ldg(brpt + k + 1);
-          int e = __ldg(brpt + k);
-          if (sorted) e = lower_bound_col(bcol, e, s1, w0);
-          for (; e < s1; ++e) {
-            const int c = __ldg(bcol + e);
-            if (sorted && c >= w1) break;
-            const unsigned d = (unsigned)(c - w0);
-            if (d < (unsigned)kWin) {
-              atomicAdd(dense + d, __dmul_rn(a, ldv(bval + e)));
-              const unsigned bit = 1u << (d & 31u);
-              if (!(bm[d >> 5] & bit)) atomicOr(bm + (d >> 5), bit);
-            }
-          }
+    int off = crpt[row];
+    bool bad = false;  // block-uniform
+    const RowSpan sp = row_span<kRankThreads>(acol, brpt, bcol, a0, a1, b_sorted != 0, ncols, sc);
+    for (long long wl = sp.lo; wl <= sp.hi; wl += kRankMaxCols) {
+      const int w0 = (int)wl;
+      const int wn = (int)min((long long)kRankMaxCols, (long long)sp.hi - wl + 1);
+      const int pl = rank_per_log2(wn);
+      const int per = 1 << pl;
+      const int t0 = threadIdx.x << pl;  // this thread's first word
+      // pass 1: distinct columns of the window
+      row_products<kRankThreads>(acol, (const VT *)nullptr, brpt, a0, a1, rq, [&](int e, double) {
+        const unsigned d = (unsigned)(__ldg(bcol + e) - w0);
+        if (d < (unsigned)wn) {
+          const unsigned bit = 1u << (d & 31u);
+          if (!(bm32[d >> 5] & bit)) atomicOr(bm32 + (d >> 5), bit);
         }
-      } else {  // one A entry per warp, lanes over the B row
-        for (int j = a0 + warp; j < a1; j += W) {
-          const int k = ld_stream(acol + j);
-          const double a = ldv_stream(aval + j);
-          const int s1 = __ldg(brpt + k + 1);
-          int e0 = __ldg(brpt + k);
-          if (sorted) e0 = lower_bound_col(bcol, e0, s1, w0);
-          for (int e = e0 + lane; e < s1; e += 32) {
-            const int c = __ldg(bcol + e);
-            if (sorted && c >= w1) break;
-            const unsigned d = (unsigned)(c - w0);
-            if (d < (unsigned)kWin) {
-              atomicAdd(dense + d, __dmul_rn(a, ldv(bval + e)));
-              const unsigned bit = 1u << (d & 31u);
-              if (!(bm[d >> 5] & bit)) atomicOr(bm + (d >> 5), bit);
-            }
-          }
-        }
-      }
+      });
       __syncthreads();
-      // compaction in column order: thread t owns bitmap word t
-      const unsigned word = threadIdx.x < kWinWords ? bm[threadIdx.x] : 0u;
-      const int pc = __popc(word);
-      int incl = pc;
+      // ranks: counts of this thread's words, scanned over the warp and the block
+      int cnt = 0;
+      for (int i = 0; i < per; ++i) cnt += __popcll(bm64[t0 + i]);
+      int incl = cnt;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const int t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
       }
-      if (lane == 31) red[warp] = incl;
+      if (lane == 31) base[warp] = incl;
       __syncthreads();
       if (warp == 0) {
-        int v = red[lane];
+        const int t = base[lane];
+        int v = t;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, v, o);
-          if (lane >= o) v += t;
+          const int u = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o) v += u;
         }
-        red[lane] = v;
+        base[lane] = v - t;
+        if (lane == 31) s_total = v;
       }
       __syncthreads();
-      const int wtot = red[W - 1];
-      int pos = off + (warp ? red[warp - 1] : 0) + incl - pc;
-      unsigned m = word;
-      if (pos + pc > row_end) {  // more entries than the symbolic count: write nothing
-        if (pc) atomicOr(err, ERR_COUNT);
-        m = 0u;
+      const int total = s_total;
+      if (!bad && off + total > row_end) {  // more columns than the symbolic count
+        bad = true;
+        if (threadIdx.x == 0) atomicOr(err, ERR_COUNT);
       }
-      while (m) {
-        const int b = __ffs(m) - 1;
-        m &= m - 1u;
-        const int d = threadIdx.x * 32 + b;
-        ccol[pos] = w0 + d;
-        cval[pos] = dense[d];
-        ++pos;
+      const bool in_smem = total <= kRankVals;
+      {
+        int p = incl - cnt;
+        int pos = off + base[warp] + p;
+        for (int i = 0; i < per; ++i) {
+          const int w = t0 + i;
+          unsigned long long m = bm64[w];
+          pre[w] = (unsigned short)p;
+          p += __popcll(m);
+          if (bad) continue;
+          while (m) {
+            const int b = __ffsll((long long)m) - 1;
+            m &= m - 1ull;
+            ccol[pos++] = w0 + (w << 6) + b;
+          }
+        }
       }
-      off += wtot;
+      if (!bad) {
+        if (in_smem) {
+          for (int i = threadIdx.x; i < total; i += kRankThreads) vals[i] = 0.0;
+        } else {
+          for (int i = threadIdx.x; i < total; i += kRankThreads) __stcg(cval + off + i, 0.0);
+        }
+      }
       __syncthreads();
+      // pass 2: values into their ranks
+      if (!bad) {
+        double *dst = in_smem ? vals : cval + off;
+        const int shift = 5 + pl;
+        row_products<kRankThreads>(acol, aval, brpt, a0, a1, rq, [&](int e, double a) {
+          const unsigned d = (unsigned)(__ldg(bcol + e) - w0);
+          if (d < (unsigned)wn) {
+            const int w = (int)(d >> 6);
+            const int rk = base[w >> shift] + pre[w] +
+                           __popcll(bm64[w] & ((1ull << (d & 63u)) - 1ull));
+            atomicAdd(dst + rk, __dmul_rn(a, ldv(bval + e)));
+          }
+        });
+      }
+      __syncthreads();
+      if (in_smem && !bad)
+        for (int i = threadIdx.x; i < total; i += kRankThreads) cval[off + i] = vals[i];
+      for (int i = 0; i < per; ++i) bm64[t0 + i] = 0ull;
+      off += total;
+      __syncthreads();  // bitmap clear and value copy-out before the next window
     }
-    if (threadIdx.x == 0 && off != row_end) atomicOr(err, ERR_COUNT);
+    if (!bad && off != row_end && threadIdx.x == 0) atomicOr(err, ERR_COUNT);
     ++rows_done;  // compensated mode: every row here is an fp64 row
   }
   if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
 }
 
-// ---- longest rows: dense fp64 accumulator in global memory ---------------------
-// Each CTA owns an ncols-long fp64 accumulator in device memory (zero between
-// rows) and a shared-memory bitmap over a 2^20-column window. Products are
-// added with global fp64 atomics (one pass over the row's products for
-// ncols <= 2^20), then the set bits are emitted in column order, each value
-// read and its slot zeroed. acc is read and written with .cg accesses (L2
-// only) so no stale L1 line is seen after another thread's atomic.
-constexpr int kDenseBits = 1 << 20;
-constexpr int kDenseWords = kDenseBits / 32;
-
 template <typename VT>
-__global__ void __launch_bounds__(kNumLongThreads)
-    k_num_long_dense(const int *__restrict__ arpt, const int *__restrict__ acol,
-                     const VT *__restrict__ aval, const int *__restrict__ brpt,
-                     const int *__restrict__ bcol, const VT *__restrict__ bval, int ncols,
-                     const int *__restrict__ crpt, int *__restrict__ ccol,
-                     double *__restrict__ cval, const int *__restrict__ rows, int count,
-                     double *__restrict__ acc_all, int *__restrict__ err,
-                     int *__restrict__ redo) {
-  extern __shared__ __align__(16) unsigned bm_dense[];
-  __shared__ int red[kNumLongThreads / 32];
-  double *acc = acc_all + (size_t)blockIdx.x * (size_t)ncols;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int W = kNumLongThreads / 32;
-  int rows_done = 0;
-  for (int r = blockIdx.x; r < count; r += gridDim.x) {
-    const int row = rows ? rows[r] : r;
-    const int a0 = arpt[row], a1 = arpt[row + 1];
-    int off = crpt[row];
-    const int row_end = crpt[row + 1];
-    for (int w0 = 0; w0 < ncols; w0 += kDenseBits) {
-      const int wn = min(kDenseBits, ncols - w0);
-      const int words = (wn + 31) >> 5;
-      for (int q = threadIdx.x; q < words; q += kNumLongThreads) bm_dense[q] = 0u;
-      __syncthreads();
-      for (int j = a0 + warp; j < a1; j += W) {
-        const int k = ld_stream(acol + j);
-        const double a = ldv_stream(aval + j);
-        const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
-        for (int e = s0 + lane; e < s1; e += 32) {
-          const int c = __ldg(bcol + e);
-          const unsigned d = (unsigned)(c - w0);
-          if (d < (unsigned)wn) {
-            atomicAdd(acc + c, __dmul_rn(a, ldv(bval + e)));
-            const unsigned bit = 1u << (d & 31u);
-            if (!(bm_dense[d >> 5] & bit)) atomicOr(bm_dense + (d >> 5), bit);
-          }
-        }
-      }
-      __threadfence_block();
-      __syncthreads();
-      // emit in column order, one round of kNumLongThreads words at a time
-      for (int base = 0; base < words; base += kNumLongThreads) {
-        const int w = base + threadIdx.x;
-        const unsigned m0 = w < words ? bm_dense[w] : 0u;
-        const int pc = __popc(m0);
-        int incl = pc;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += t;
-        }
-        if (lane == 31) red[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-          int v = red[lane];
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += t;
-          }
-          red[lane] = v;
-        }
-        __syncthreads();
-        const int rtot = red[W - 1];
-        int pos = off + (warp ? red[warp - 1] : 0) + incl - pc;
-        unsigned m = m0;
-        if (pos + pc > row_end) {  // more entries than the symbolic count: write nothing
-          if (pc) atomicOr(err, ERR_COUNT);
-          m = 0u;
-        }
-        while (m) {
-          const int b = __ffs(m) - 1;
-          m &= m - 1u;
-          const int c = w0 + w * 32 + b;
-          ccol[pos] = c;
-          cval[pos] = __ldcg(acc + c);
-          __stcg(acc + c, 0.0);
-          ++pos;
-        }
-        off += rtot;
-        __syncthreads();
-      }
-    }
-    if (threadIdx.x == 0 && off != row_end) atomicOr(err, ERR_COUNT);
-    ++rows_done;
-  }
-  if (redo && threadIdx.x == 0 && rows_done) atomicAdd(redo, rows_done);
+static cudaError_t run_num_rank(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
+                                bool b_sorted, const int *crpt, int *ccol, double *cval,
+                                const int *rows, int count, int *err, int *redo, int *ticket,
+                                cudaStream_t s) {
+  const int pl = rank_per_log2((int)std::min<long long>(B.ncols, kRankMaxCols));
+  const int smem = rank_smem(pl);
+  const void *f = (const void *)k_num_rank<VT>;
+  const int grid = persistent_grid(f, kRankThreads, smem, count, 1);
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  k_num_rank<VT><<<grid, kRankThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, B.ncols,
+                                                  b_sorted ? 1 : 0, pl, crpt, ccol, cval, rows,
+                                                  count, err, redo, ticket);
+  return cudaGetLastError();
 }
 
 // ---- dispatch ------------------------------------------------------------------------
@@ -644,14 +589,14 @@ static cudaError_t num_group_bin(int bin, const CsrDev &A, const CsrDev &B, cons
 template <int LOG2T, typename VT>
 static cudaError_t run_num_block(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
                                  const int *crpt, int *ccol, double *cval, const int *rows,
-                                 int count, int *err, int *redo, cudaStream_t s) {
+                                 int count, int *err, int *redo, int *ticket, cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
   const int smem = T * 12 + (T / 2) * 12 + (T / 2) * 4;
   const void *f = (const void *)k_num_block<LOG2T, VT>;
   const int grid = persistent_grid(f, kNumBlockThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   k_num_block<LOG2T, VT><<<grid, kNumBlockThreads, smem, s>>>(
-      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, redo);
+      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, redo, ticket);
   return cudaGetLastError();
 }
 
@@ -659,7 +604,7 @@ template <typename VT, bool COMP>
 static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, const CsrDev &A,
                                  const CsrDev &B, const VT *av, const VT *bv, const int *crpt,
                                  int *ccol, double *cval, const int *rows, int count, int *err,
-                                 CompArgs comp, cudaStream_t s) {
+                                 CompArgs comp, int *ticket, cudaStream_t s) {
   if (bin < kNumGroupBins) {
 #define NSPB_GB(GL, OW) \
   num_group_bin<GL, OW, VT, COMP>(bin, A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
@@ -674,67 +619,41 @@ static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, 
 #undef NSPB_GB
   }
   int *redo = COMP ? comp.redo : nullptr;
+  if (bin >= kRankFromBin)
+    return run_num_rank<VT>(A, B, av, bv, b_sorted, crpt, ccol, cval, rows, count, err, redo,
+                            ticket, s);
   switch (bin) {
     case kNumGroupBins:
-      return run_num_block<11, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
+      return run_num_block<11, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo,
+                                  ticket, s);
     case kNumGroupBins + 1:
-      return run_num_block<12, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
-    case kNumGroupBins + 2:
-      return run_num_block<13, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo, s);
-    default: {
-      // dense accumulator per CTA when its footprint fits kDenseBudget,
-      // else shared-memory column windows
-      const int dsmem = kDenseWords * 4;
-      const void *fd = (const void *)k_num_long_dense<VT>;
-      int grid = persistent_grid(fd, kNumLongThreads, dsmem, count, 1);
-      const long long per_cta = 8LL * (B.ncols > 0 ? B.ncols : 1);
-      const long long fit = kDenseBudget / per_cta;
-      if (grid > 0 && fit >= 1) {
-        grid = (int)std::min<long long>(grid, fit);
-        double *acc = nullptr;
-        if (scratch_alloc(reinterpret_cast<void **>(&acc), (size_t)per_cta * grid, s) == NSPB_OK) {
-          cudaError_t e = cudaMemsetAsync(acc, 0, (size_t)per_cta * grid, s);
-          if (e == cudaSuccess) {
-            k_num_long_dense<VT><<<grid, kNumLongThreads, dsmem, s>>>(
-                A.rpt, A.col, av, B.rpt, B.col, bv, B.ncols, crpt, ccol, cval, rows, count, acc,
-                err, redo);
-            e = cudaGetLastError();
-          }
-          scratch_free(acc, s);
-          return e;
-        }
-      }
-      const int smem = kWin * 8 + kWinWords * 4;
-      const void *f = (const void *)k_num_long<VT>;
-      grid = persistent_grid(f, kNumLongThreads, smem, count, 1);
-      if (grid <= 0) return cudaErrorInvalidConfiguration;
-      k_num_long<VT><<<grid, kNumLongThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv,
-                                                         B.ncols, b_sorted, crpt, ccol, cval,
-                                                         rows, count, err, redo);
-      return cudaGetLastError();
-    }
+      return run_num_block<12, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo,
+                                  ticket, s);
+    default:
+      return run_num_block<13, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo,
+                                  ticket, s);
   }
 }
 
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
                                const CsrDev &A, const CsrDev &B, const int *crpt,
                                int *ccol, double *cval, const int *rows, int count,
-                               int *err, cudaStream_t s) {
+                               int *err, int *ticket, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   return numeric_bin_t<double, false>(bin, lanes, owned, b_sorted, A, B, A.val, B.val, crpt,
                                       ccol, cval, rows, count, err, CompArgs{0, nullptr, nullptr},
-                                      s);
+                                      ticket, s);
 }
 
 cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorted,
                                     const CsrDev &A, const CsrDev &B, const int *crpt,
                                     int *ccol, double *cval, const int *rows, int count,
                                     int nmax, int *redo, int *max_deg, int *err,
-                                    cudaStream_t s) {
+                                    int *ticket, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   return numeric_bin_t<float, true>(bin, lanes, owned, b_sorted, A, B, A.val32, B.val32, crpt,
                                     ccol, cval, rows, count, err, CompArgs{nmax, redo, max_deg},
-                                    s);
+                                    ticket, s);
 }
 
 }  // namespace nspb

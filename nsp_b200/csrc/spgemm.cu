@@ -250,8 +250,8 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   for (int b = 0; b < kSymBins; ++b) {
     const int c = h.sym_counts[b];
     if (c <= 0) continue;
-    e = launch_symbolic_bin(b, lanes, A, B, direct ? nullptr : perm + off.v[b], c, row_nz,
-                            &ctr->err, s);
+    e = launch_symbolic_bin(b, lanes, b_sorted, A, B, direct ? nullptr : perm + off.v[b], c,
+                            row_nz, &ctr->err, &ctr->ticket[b], s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
@@ -288,10 +288,12 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     const int c = h.num_counts[b];
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
+    int *ticket = &ctr->ticket[16 + b];
     e = comp ? launch_numeric_comp_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows,
-                                       c, nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
+                                       c, nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err,
+                                       ticket, s)
              : launch_numeric_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows, c,
-                                  &ctr->err, s);
+                                  &ctr->err, ticket, s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }

@@ -25,6 +25,8 @@ struct DevCounters {
   float max_row_err;
   int max_comp_deg;  // compensated mode: largest A-row degree of a pair row
   int pad[2];
+  int ticket[32];    // row tickets of the block-per-row launches (symbolic
+                     // bin b at b, numeric bin b at 16 + b)
 };
 
 struct HostStage {

@@ -6,14 +6,17 @@
 //   nsp_set_row_nz_bin_each_tb_max   :863-915  (48 KB mod-hash table)
 //   nsp_set_row_nz_bin_each_tb_large :755-859  + _chunk :592-750 (fail list,
 //                                     column windows for the longest rows)
-// Here every kernel is a persistent grid-stride loop over its bin's rows, so
-// one launch covers a bin whatever its size, tables are sized to the bin
-// (up to 128 KB per block on sm_100), and the longest rows count distinct
-// columns in a 2^20-bit shared-memory bitmap per column window instead of a
-// hash table with a fail-and-retry path.
+// Here every kernel is persistent, so one launch covers a bin whatever its
+// size. Rows of up to 3072 intermediate products use row groups with hash
+// tables sized to the bin; longer rows take a whole block each (handed out by
+// a ticket counter as blocks free up) and count distinct columns as bits of a
+// shared-memory bitmap over the row's own column span instead of a hash table
+// with a fail-and-retry path.
 #include "common.cuh"
 #include "internal.h"
 #include "launch_util.h"
+
+#include <algorithm>
 
 namespace nspb {
 
@@ -67,88 +70,80 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// ---- one block per row: 16 warps over the A entries, one shared table ---------
-constexpr int kSymBlockThreads = 512;
-
-template <int LOG2T>
-__global__ void __launch_bounds__(kSymBlockThreads)
-    k_sym_block(const int *__restrict__ arpt, const int *__restrict__ acol,
-                const int *__restrict__ brpt, const int *__restrict__ bcol,
-                const int *__restrict__ rows, int count, int *__restrict__ row_nz,
-                int *__restrict__ err) {
-  constexpr int T = 1 << LOG2T;
-  extern __shared__ __align__(16) int smem_sym[];
-  int *table = smem_sym;
-  __shared__ int red[kSymBlockThreads / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int W = kSymBlockThreads / 32;
-  for (int r = blockIdx.x; r < count; r += gridDim.x) {
-    const int row = rows ? rows[r] : r;
-    for (int s = threadIdx.x; s < T; s += kSymBlockThreads) table[s] = kEmpty;
-    __syncthreads();
-    const int a0 = arpt[row], a1 = arpt[row + 1];
-    int nz = 0;
-    for (int j = a0 + warp; j < a1; j += W) {
-      const int k = ld_stream(acol + j);
-      const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
-      for (int e = s0 + lane; e < s1; e += 32) nz += sym_insert<LOG2T>(table, __ldg(bcol + e), err);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nz += __shfl_xor_sync(0xffffffffu, nz, o);
-    if (lane == 0) red[warp] = nz;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int s = 0;
-#pragma unroll
-      for (int w = 0; w < W; ++w) s += red[w];
-      row_nz[row] = s;
-    }
-    __syncthreads();
-  }
-}
-
-// ---- longest rows: distinct columns as bits of a 2^20-column window ----------
-constexpr int kLongThreads = 1024;
+// ---- rows of 6K intermediate products and more: one block per row -------------
+// Distinct columns are counted as set bits of a shared-memory bitmap over the
+// row's column span [lo, hi] (see row_span), in windows of 2^20 columns. A
+// row whose span is wider than one window but whose products fit a 2^15-slot
+// hash table at load <= 0.75 is counted in that table instead (same shared
+// memory), so it takes one pass over its products rather than one per window.
+// A block-diagonal batch of products, whose B has the columns of every
+// product, thus costs each row only its own span.
+constexpr int kWideThreads = 1024;
 constexpr int kLongBits = 1 << 20;  // 128 KB of shared memory
 constexpr int kLongWords = kLongBits / 32;
+constexpr int kWideLog2T = 15;      // hash table of 2^15 ints: the same 128 KB
+constexpr int kWideHashMax = 3 << (kWideLog2T - 2);
 
-__global__ void __launch_bounds__(kLongThreads)
-    k_sym_long(const int *__restrict__ arpt, const int *__restrict__ acol,
-               const int *__restrict__ brpt, const int *__restrict__ bcol,
-               int ncols, const int *__restrict__ rows, int count,
-               int *__restrict__ row_nz) {
+__global__ void __launch_bounds__(kWideThreads)
+    k_sym_wide(const int *__restrict__ arpt, const int *__restrict__ acol,
+               const int *__restrict__ brpt, const int *__restrict__ bcol, int ncols,
+               int b_sorted, const int *__restrict__ rows, int count,
+               int *__restrict__ row_nz, int *__restrict__ err, int *__restrict__ ticket) {
   extern __shared__ __align__(16) unsigned bm[];
-  __shared__ int red[kLongThreads / 32];
+  __shared__ int red[kWideThreads / 32];
+  __shared__ int s_slot;
+  __shared__ RowQueue<kWideThreads> rq;
+  __shared__ SpanScratch<kWideThreads> sc;
+  row_queue_init(rq);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int W = kLongThreads / 32;
-  for (int r = blockIdx.x; r < count; r += gridDim.x) {
+  constexpr int W = kWideThreads / 32;
+  // block sum of c, valid in every thread; ends with a barrier
+  auto block_sum = [&](int c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) red[warp] = c;
+    __syncthreads();
+    int t = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) t += red[w];
+    __syncthreads();
+    return t;
+  };
+  for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
     const int a0 = arpt[row], a1 = arpt[row + 1];
+    const RowSpan sp = row_span<kWideThreads>(acol, brpt, bcol, a0, a1, b_sorted != 0, ncols, sc);
     int total = 0;
-    for (int c0 = 0; c0 < ncols; c0 += kLongBits) {
-      for (int s = threadIdx.x; s < kLongWords; s += kLongThreads) bm[s] = 0u;
+    if ((long long)sp.hi - sp.lo + 1 > kLongBits && sp.ip <= kWideHashMax) {
+      int *table = reinterpret_cast<int *>(bm);
+      for (int q = threadIdx.x; q < (1 << kWideLog2T); q += kWideThreads) table[q] = kEmpty;
       __syncthreads();
-      for (int j = a0 + warp; j < a1; j += W) {
-        const int k = ld_stream(acol + j);
-        const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
-        for (int e = s0 + lane; e < s1; e += 32) {
-          const unsigned d = (unsigned)(__ldg(bcol + e) - c0);
-          if (d < (unsigned)kLongBits) {
-            const unsigned bit = 1u << (d & 31u);
-            if (!(bm[d >> 5] & bit)) atomicOr(&bm[d >> 5], bit);
-          }
-        }
+      int nz = 0;
+      row_products<kWideThreads>(acol, (const double *)nullptr, brpt, a0, a1, rq,
+                                 [&](int e, double) {
+                                   nz += sym_insert<kWideLog2T>(table, __ldg(bcol + e), err);
+                                 });
+      total = block_sum(nz);
+    } else {
+      for (long long w0 = sp.lo; w0 <= sp.hi; w0 += kLongBits) {
+        const int wn = (int)min((long long)kLongBits, (long long)sp.hi - w0 + 1);
+        const int words = (wn + 31) >> 5;
+        const int base = (int)w0;
+        for (int q = threadIdx.x; q < words; q += kWideThreads) bm[q] = 0u;
+        __syncthreads();
+        row_products<kWideThreads>(acol, (const double *)nullptr, brpt, a0, a1, rq,
+                                   [&](int e, double) {
+                                     const unsigned d = (unsigned)(__ldg(bcol + e) - base);
+                                     if (d < (unsigned)wn) {
+                                       const unsigned bit = 1u << (d & 31u);
+                                       if (!(bm[d >> 5] & bit)) atomicOr(&bm[d >> 5], bit);
+                                     }
+                                   });
+        __syncthreads();
+        int c = 0;
+        for (int q = threadIdx.x; q < words; q += kWideThreads) c += __popc(bm[q]);
+        total += block_sum(c);
       }
-      __syncthreads();
-      int c = 0;
-      for (int s = threadIdx.x; s < kLongWords; s += kLongThreads) c += __popc(bm[s]);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-      if (lane == 0) red[warp] = c;
-      __syncthreads();
-      if (threadIdx.x == 0)
-        for (int w = 0; w < W; ++w) total += red[w];
-      __syncthreads();
     }
     if (threadIdx.x == 0) row_nz[row] = total;
   }
@@ -182,41 +177,25 @@ static cudaError_t sym_group_bin(int bin, const CsrDev &A, const CsrDev &B, cons
   }
 }
 
-template <int LOG2T>
-static cudaError_t run_sym_block(const CsrDev &A, const CsrDev &B, const int *rows, int count,
-                                 int *row_nz, int *err, cudaStream_t s) {
-  const int smem = (1 << LOG2T) * 4;
-  const void *f = (const void *)k_sym_block<LOG2T>;
-  const int grid = persistent_grid(f, kSymBlockThreads, smem, count, 1);
-  if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_block<LOG2T><<<grid, kSymBlockThreads, smem, s>>>(A.rpt, A.col, B.rpt, B.col, rows,
-                                                          count, row_nz, err);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_symbolic_bin(int bin, int lanes, const CsrDev &A, const CsrDev &B,
-                                const int *rows, int count, int *row_nz, int *err,
-                                cudaStream_t s) {
+cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const CsrDev &A,
+                                const CsrDev &B, const int *rows, int count, int *row_nz,
+                                int *err, int *ticket, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin < kSymGroupBins) {
     if (lanes == 8) return sym_group_bin<8>(bin, A, B, rows, count, row_nz, err, s);
     if (lanes == 16) return sym_group_bin<16>(bin, A, B, rows, count, row_nz, err, s);
     return sym_group_bin<32>(bin, A, B, rows, count, row_nz, err, s);
   }
-  switch (bin) {
-    case kSymGroupBins: return run_sym_block<13>(A, B, rows, count, row_nz, err, s);
-    case kSymGroupBins + 1: return run_sym_block<14>(A, B, rows, count, row_nz, err, s);
-    case kSymGroupBins + 2: return run_sym_block<15>(A, B, rows, count, row_nz, err, s);
-    default: {
-      const int smem = kLongWords * 4;
-      const void *f = (const void *)k_sym_long;
-      const int grid = persistent_grid(f, kLongThreads, smem, count, 1);
-      if (grid <= 0) return cudaErrorInvalidConfiguration;
-      k_sym_long<<<grid, kLongThreads, smem, s>>>(A.rpt, A.col, B.rpt, B.col, B.ncols, rows,
-                                                  count, row_nz);
-      return cudaGetLastError();
-    }
-  }
+  // the bitmap covers one window of B's columns at most; the hash table needs
+  // the full 128 KB, which it only uses when B has more columns than a window
+  const int smem = (int)std::min<long long>(kLongWords, ((long long)B.ncols + 31) >> 5) * 4;
+  const void *f = (const void *)k_sym_wide;
+  const int grid = persistent_grid(f, kWideThreads, smem, count, 1);
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  k_sym_wide<<<grid, kWideThreads, smem, s>>>(A.rpt, A.col, B.rpt, B.col, B.ncols,
+                                              b_sorted ? 1 : 0, rows, count, row_nz, err,
+                                              ticket);
+  return cudaGetLastError();
 }
 
 }  // namespace nspb

@@ -131,6 +131,34 @@ def test_unsorted_long_rows(cuda):
     check(P, Pu)
 
 
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_wide_span_rows(cuda, shuffle):
+    # B's columns spread over 3M: the long rows' spans cover several 2^20-column
+    # windows, rows of 6K..24K products take the symbolic hash table, rows of
+    # 4K..6K entries accumulate in shared memory window by window, longer ones
+    # in C.val; shuffled B rows make every span [0, ncols)
+    rng = np.random.default_rng(17)
+    ncols, nbr, per = 3_000_000, 2000, 25
+    pool = np.sort(rng.choice(ncols, 150_000, replace=False))
+    bcol = np.concatenate([np.sort(rng.choice(pool, per, replace=False))
+                           for _ in range(nbr)]).astype(np.int32)
+    brp = (np.arange(nbr + 1) * per).astype(np.int32)
+    if shuffle:
+        for i in range(nbr):
+            rng.shuffle(bcol[brp[i]:brp[i + 1]])
+    B = HostCSR(nbr, ncols, brp, bcol, rng.uniform(-1, 1, len(bcol)))
+    deg = np.linspace(100, 2000, 60).astype(np.int64)
+    arp = np.zeros(len(deg) + 1, np.int32)
+    arp[1:] = np.cumsum(deg)
+    acol = np.concatenate([np.sort(rng.choice(nbr, d, replace=False)) for d in deg])
+    A = HostCSR(len(deg), nbr, arp, acol.astype(np.int32), rng.uniform(-1, 1, int(arp[-1])))
+    got, st = check(A, B)
+    assert st["b_sorted"] == (0 if shuffle else 1)
+    assert sum(st["sym_bins"][8:11]) > 0 and st["sym_bins"][11] > 0
+    nz = np.diff(got.rowptr)
+    assert np.any((nz > 4096) & (nz <= 6144)) and np.any(nz > 6144)
+
+
 def test_two_call_matches_one_call(cuda):
     A = nb.gen.random(4000, 3000, 0, 50, seed=31)
     B = nb.gen.random(3000, 3500, 0, 50, seed=32)
