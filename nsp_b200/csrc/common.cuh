@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace cg = cooperative_groups;
 
 namespace nspb {
@@ -194,34 +196,64 @@ __device__ __forceinline__ void row_queue_init(RowQueue<THREADS> &rq) {
 // whatever the lengths of the B rows it touches (power-law matrices mix rows
 // of one entry with hub rows of 10^4 and more). The A row is taken in rounds
 // of THREADS entries, one per thread:
-//   - a B row of at most 32 entries (4 when the round holds fewer than
-//     THREADS/4 entries) is walked by its thread: up to THREADS independent
-//     gather chains in flight;
+//   - a B row of at most kRowSmall entries (4 when the round holds fewer than
+//     THREADS/4 entries) is walked by its thread, four entries' loads at a
+//     time: up to THREADS independent gather chains in flight;
 //   - a longer B row goes to a queue; warps take queued rows one at a time
 //     from a shared cursor, lanes over the row's entries;
 //   - a B row of THREADS entries or more is walked by the whole block, thread
 //     t taking the products whose index in the round's concatenation of such
 //     rows is t mod THREADS.
-// f(e, a) gets the B entry index and the A value (0 when aval is null). Every
-// thread of the block must call this with the same (a0, a1) after a block
-// barrier, and a block barrier must separate two calls.
+// f(c, a, b) gets the B entry's column, the A value and the B value (values 0
+// when aval / bval are null). Every thread of the block must call this with
+// the same (a0, a1) after a block barrier, and a block barrier must separate
+// two calls.
+#ifndef NSPB_ROW_SMALL
+#define NSPB_ROW_SMALL 16
+#endif
+constexpr int kRowSmall = NSPB_ROW_SMALL;  // longest B row one thread walks alone
+
 template <int THREADS, typename VT, typename F>
 __device__ __forceinline__ void row_products(const int *__restrict__ acol,
                                              const VT *__restrict__ aval,
-                                             const int *__restrict__ brpt, int a0, int a1,
+                                             const int *__restrict__ brpt,
+                                             const int *__restrict__ bcol,
+                                             const VT *__restrict__ bval, int a0, int a1,
                                              RowQueue<THREADS> &rq, F &&f) {
   static_assert((THREADS & (THREADS - 1)) == 0, "THREADS must be a power of two");
   const int lane = threadIdx.x & 31;
+  auto bv = [&](int e) -> double { return bval ? ldv(bval + e) : 0.0; };
+  // entries [e, end) with stride S, two loads in flight per thread
+  auto strided = [&](int e, int end, double a, auto S) {
+    constexpr int kS = decltype(S)::value;
+    for (; e + kS < end; e += 2 * kS) {
+      const int c0 = __ldg(bcol + e), c1 = __ldg(bcol + e + kS);
+      const double b0 = bv(e), b1 = bv(e + kS);
+      f(c0, a, b0);
+      f(c1, a, b1);
+    }
+    if (e < end) f(__ldg(bcol + e), a, bv(e));
+  };
   int par = 0;
   for (int jr = a0; jr < a1; jr += THREADS, par ^= 1) {  // uniform across the block
-    const int small_max = min(THREADS, a1 - jr) * 4 >= THREADS ? 32 : 4;
+    const int small_max = min(THREADS, a1 - jr) * 4 >= THREADS ? kRowSmall : 4;
     const int j = jr + (int)threadIdx.x;
     if (j < a1) {
       const int k = ld_stream(acol + j);
       const double a = aval ? ldv_stream(aval + j) : 0.0;
       const int s0 = __ldg(brpt + k), s1 = __ldg(brpt + k + 1);
       if (s1 - s0 <= small_max) {
-        for (int e = s0; e < s1; ++e) f(e, a);
+        int e = s0;
+        for (; e + 4 <= s1; e += 4) {
+          const int c0 = __ldg(bcol + e), c1 = __ldg(bcol + e + 1);
+          const int c2 = __ldg(bcol + e + 2), c3 = __ldg(bcol + e + 3);
+          const double b0 = bv(e), b1 = bv(e + 1), b2 = bv(e + 2), b3 = bv(e + 3);
+          f(c0, a, b0);
+          f(c1, a, b1);
+          f(c2, a, b2);
+          f(c3, a, b3);
+        }
+        for (; e < s1; ++e) f(__ldg(bcol + e), a, bv(e));
       } else {
         const int big = (s1 - s0 >= THREADS) ? 1 : 0;
         const int slot = atomicAdd(&rq.ctr[par][big], 1);
@@ -240,15 +272,14 @@ __device__ __forceinline__ void row_products(const int *__restrict__ acol,
       i = __shfl_sync(0xffffffffu, i, 0);
       if (i >= nm) break;
       const int4 v = rq.q[i];
-      const double a = __hiloint2double(v.w, v.z);
-      for (int e = v.x + lane; e < v.y; e += 32) f(e, a);
+      strided(v.x + lane, v.y, __hiloint2double(v.w, v.z), std::integral_constant<int, 32>());
     }
     unsigned pos = 0;  // products of the long rows before row i, mod 2^32
     for (int i = 0; i < nb; ++i) {
       const int4 v = rq.q[THREADS - 1 - i];
-      const double a = __hiloint2double(v.w, v.z);
       const int first = (int)((threadIdx.x - pos) & (unsigned)(THREADS - 1));
-      for (int e = v.x + first; e < v.y; e += THREADS) f(e, a);
+      strided(v.x + first, v.y, __hiloint2double(v.w, v.z),
+              std::integral_constant<int, THREADS>());
       pos += (unsigned)(v.y - v.x);
     }
     __syncthreads();

@@ -307,9 +307,9 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     __syncthreads();
     const int a0 = arpt[row], a1 = arpt[row + 1];
     int mn = 0x7fffffff, mx = -1;
-    row_products<kNumBlockThreads>(acol, aval, brpt, a0, a1, rq, [&](int e, double a) {
-      const int key = __ldg(bcol + e);
-      num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, ldv(bval + e)), err);
+    row_products<kNumBlockThreads>(acol, aval, brpt, bcol, bval, a0, a1, rq,
+                                   [&](int key, double a, double b) {
+      num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, b), err);
       mn = min(mn, key);
       mx = max(mx, key);
     });
@@ -450,8 +450,9 @@ __global__ void __launch_bounds__(kRankThreads)
       const int per = 1 << pl;
       const int t0 = threadIdx.x << pl;  // this thread's first word
       // pass 1: distinct columns of the window
-      row_products<kRankThreads>(acol, (const VT *)nullptr, brpt, a0, a1, rq, [&](int e, double) {
-        const unsigned d = (unsigned)(__ldg(bcol + e) - w0);
+      row_products<kRankThreads>(acol, (const VT *)nullptr, brpt, bcol, (const VT *)nullptr, a0,
+                                 a1, rq, [&](int c, double, double) {
+        const unsigned d = (unsigned)(c - w0);
         if (d < (unsigned)wn) {
           const unsigned bit = 1u << (d & 31u);
           if (!(bm32[d >> 5] & bit)) atomicOr(bm32 + (d >> 5), bit);
@@ -515,13 +516,14 @@ __global__ void __launch_bounds__(kRankThreads)
       if (!bad) {
         double *dst = in_smem ? vals : cval + off;
         const int shift = 5 + pl;
-        row_products<kRankThreads>(acol, aval, brpt, a0, a1, rq, [&](int e, double a) {
-          const unsigned d = (unsigned)(__ldg(bcol + e) - w0);
+        row_products<kRankThreads>(acol, aval, brpt, bcol, bval, a0, a1, rq,
+                                   [&](int c, double a, double b) {
+          const unsigned d = (unsigned)(c - w0);
           if (d < (unsigned)wn) {
             const int w = (int)(d >> 6);
             const int rk = base[w >> shift] + pre[w] +
                            __popcll(bm64[w] & ((1ull << (d & 63u)) - 1ull));
-            atomicAdd(dst + rk, __dmul_rn(a, ldv(bval + e)));
+            atomicAdd(dst + rk, __dmul_rn(a, b));
           }
         });
       }

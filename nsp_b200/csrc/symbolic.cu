@@ -119,9 +119,10 @@ __global__ void __launch_bounds__(kWideThreads)
       for (int q = threadIdx.x; q < (1 << kWideLog2T); q += kWideThreads) table[q] = kEmpty;
       __syncthreads();
       int nz = 0;
-      row_products<kWideThreads>(acol, (const double *)nullptr, brpt, a0, a1, rq,
-                                 [&](int e, double) {
-                                   nz += sym_insert<kWideLog2T>(table, __ldg(bcol + e), err);
+      row_products<kWideThreads>(acol, (const double *)nullptr, brpt, bcol,
+                                 (const double *)nullptr, a0, a1, rq,
+                                 [&](int c, double, double) {
+                                   nz += sym_insert<kWideLog2T>(table, c, err);
                                  });
       total = block_sum(nz);
     } else {
@@ -131,9 +132,10 @@ __global__ void __launch_bounds__(kWideThreads)
         const int base = (int)w0;
         for (int q = threadIdx.x; q < words; q += kWideThreads) bm[q] = 0u;
         __syncthreads();
-        row_products<kWideThreads>(acol, (const double *)nullptr, brpt, a0, a1, rq,
-                                   [&](int e, double) {
-                                     const unsigned d = (unsigned)(__ldg(bcol + e) - base);
+        row_products<kWideThreads>(acol, (const double *)nullptr, brpt, bcol,
+                                   (const double *)nullptr, a0, a1, rq,
+                                   [&](int c, double, double) {
+                                     const unsigned d = (unsigned)(c - base);
                                      if (d < (unsigned)wn) {
                                        const unsigned bit = 1u << (d & 31u);
                                        if (!(bm[d >> 5] & bit)) atomicOr(&bm[d >> 5], bit);
