@@ -50,7 +50,8 @@ typedef enum {
                               bounded wait exhausted); results are invalid      */
   NSPB_ERR_NO_DEVICE = -6, /* no CUDA device visible                            */
   NSPB_ERR_UNSUPPORTED = -7,
-  NSPB_ERR_CAPACITY = -8   /* a size exceeds a fixed capacity of the call       */
+  NSPB_ERR_CAPACITY = -8,  /* a size exceeds a fixed capacity of the call       */
+  NSPB_ERR_IO = -9         /* a file could not be opened, read or written       */
 } nspb_status;
 
 /* value types */
@@ -237,6 +238,44 @@ int64_t nspb_gen_random(int32_t nrows, int32_t ncols, int32_t dmin,
                         int32_t *rowptr, int32_t *col, double *val);
 /* Lower bound x_min of the truncated Pareto used by nspb_gen_powerlaw.       */
 double nspb_powerlaw_xmin(double alpha, double mean_deg, int32_t max_deg);
+
+/* ---- matrix files (host memory) ---------------------------------------------
+ * The reference's own formats, so its data files drive this library:
+ *  - binary COO (src/READ_MATRIX_MPI.cpp:146-356, read through
+ *    load_MatrixMPI, src/distribute.cu:1071-1125): a header of int64
+ *    {nr, nc, nt} (header_type 1) or {nr, nt} (header_type 0, nc = nr), then
+ *    nt records {ii, jj, aa}: 1-based row and column as int64
+ *    (index_bytes 8, what main.cu loads) or int32 (index_bytes 4), and an fp64
+ *    value; records sorted by row;
+ *  - the same as text (READ_ASCII_MATRIX_MPI, src/READ_MATRIX_MPI.cpp:365):
+ *    '%' comment lines, a line "nr nc nt" or "nr nt", then "ii jj aa" lines.
+ * As the reference does for one rank, local row 0 is the first row that holds
+ * an entry and nrows = last row - first row + 1 (first_row gives the offset;
+ * full_nrows is the header's nr), and a row whose columns are out of order is
+ * stably sorted by column (src/distribute.cu:1051-1069). Duplicates are kept. */
+typedef struct {
+  int64_t nrows, ncols, nnz;
+  int64_t full_nrows;  /* nr of the header                                  */
+  int64_t first_row;   /* 0-based file row of local row 0                   */
+  int32_t *rowptr;     /* [nrows+1]; library-allocated, see nspb_host_csr_free */
+  int32_t *col;        /* [nnz], 0-based                                     */
+  double *val;         /* [nnz]                                              */
+} nspb_host_csr;
+
+int nspb_read_coo_bin(const char *path, int header_type, int index_bytes,
+                      nspb_host_csr *out);
+int nspb_read_coo_ascii(const char *path, nspb_host_csr *out);
+void nspb_host_csr_free(nspb_host_csr *m);
+/* Binary COO writer of main.cu:468-512 (write_binary_matrix<mtype, otype>):
+ * header {nr, nc} as int32 (index_bytes 4) or int64 (8), then nt as int64;
+ * records {ii, jj} 1-based in the same width, then the fp64 value. With
+ * index_bytes 4 the header is 16 bytes, which the binary reader above (like
+ * the reference's) does not accept; index_bytes 8 round-trips.             */
+int nspb_write_coo_bin(const char *path, const int32_t *rowptr, const int32_t *col,
+                       const double *val, int64_t nrows, int64_t ncols, int index_bytes);
+/* MatrixMarket coordinate writer of src/matrixIO.cu:299-339 (1-based).    */
+int nspb_write_mtx(const char *path, const int32_t *rowptr, const int32_t *col,
+                   const double *val, int64_t nrows, int64_t ncols);
 
 #ifdef __cplusplus
 }

@@ -13,14 +13,14 @@ from __future__ import annotations
 
 import ctypes as C
 
-from . import gen
+from . import gen, matio
 from ._lib import (F32, F64, PREC_FP32_COMP, PREC_FP64, CsrIn, CsrOut, NspbError, Opts,
                    SfCSR, Stats, check, lib)
 from .csr import DeviceCSR, HostCSR, adopt
 
 __all__ = ["spgemm", "spgemm_symbolic", "spgemm_numeric", "intprod", "nsp_spgemm_kernel_hash",
            "nsparseMGPU_version1", "DeviceCSR", "HostCSR", "gen", "NspbError", "lib",
-           "make_opts", "stats_dict"]
+           "make_opts", "stats_dict", "matio"]
 
 
 def _stream_ptr(stream):

@@ -29,6 +29,7 @@ ERR_DEVICE = -5
 ERR_NO_DEVICE = -6
 ERR_UNSUPPORTED = -7
 ERR_CAPACITY = -8
+ERR_IO = -9
 
 F64 = 0
 F32 = 1
@@ -62,6 +63,13 @@ class Stats(C.Structure):
                 ("max_row_err", C.c_double), ("launches", C.c_int32),
                 ("ms_rowinfo", C.c_float), ("ms_symbolic", C.c_float),
                 ("ms_scan", C.c_float), ("ms_numeric", C.c_float), ("_pad", C.c_float)]
+
+
+class HostCsr(C.Structure):
+    """nspb_host_csr: a CSR in host memory allocated by the library."""
+    _fields_ = [("nrows", C.c_int64), ("ncols", C.c_int64), ("nnz", C.c_int64),
+                ("full_nrows", C.c_int64), ("first_row", C.c_int64),
+                ("rowptr", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p)]
 
 
 class SfCSR(C.Structure):
@@ -110,6 +118,13 @@ _SIGS = {
                                     C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nspb_powerlaw_xmin": (C.c_double, [C.c_double, C.c_double, C.c_int32]),
     "nspb_nsp_spgemm_kernel_hash": (C.c_int, [P(SfCSR), P(SfCSR), P(SfCSR)]),
+    "nspb_read_coo_bin": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(HostCsr)]),
+    "nspb_read_coo_ascii": (C.c_int, [C.c_char_p, P(HostCsr)]),
+    "nspb_host_csr_free": (None, [P(HostCsr)]),
+    "nspb_write_coo_bin": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                     C.c_int64, C.c_int]),
+    "nspb_write_mtx": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                 C.c_int64]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -397,6 +397,7 @@ const char *nspb_strerror(int status) {
     case NSPB_ERR_NO_DEVICE: return "no CUDA device";
     case NSPB_ERR_UNSUPPORTED: return "unsupported";
     case NSPB_ERR_CAPACITY: return "output capacity too small";
+    case NSPB_ERR_IO: return "file could not be opened, read or written";
     default: return "unknown status";
   }
 }
