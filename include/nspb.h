@@ -209,6 +209,26 @@ int nspb_spgemm_rowblocked(const nspb_csr_in *A, const nspb_csr_in *B,
                            int64_t *nnz_out, int32_t *nblocks_out,
                            const nspb_opts *opts);
 
+/* ---- AMG Galerkin driver ----------------------------------------------------
+ * T = A^T (CSRm::T, src/CSR.cu:738-785, cuSPARSE csr2csc there): every row of
+ * T lists its columns (A's rows) ascending, duplicates in their stored order.
+ * fp64 or fp32 values (T keeps A's value type; T->val then holds floats).
+ * Output allocation follows nspb_spgemm (NULL arrays are cudaMalloc'ed;
+ * caller arrays must hold nnz(A) entries, else NSPB_ERR_CAPACITY).          */
+int nspb_transpose(const nspb_csr_in *A, nspb_csr_out *T, const nspb_opts *opts);
+/* Smoothed-aggregation prolongator P = P_tent - omega D^-1 (A P_tent), D the
+ * diagonal of A (CSRm::diag, src/CSR.cu:1389-1418: the last stored diagonal
+ * entry of a row). fp64; A square with every diagonal entry stored. Each
+ * value is (-omega * (A P_tent)_ij) / d_i, plus P_tent_ij where P_tent has an
+ * entry, rounded in that order. NSPB_ERR_INVALID when a diagonal entry is
+ * missing.                                                                   */
+int nspb_sa_prolongator(const nspb_csr_in *A, const nspb_csr_in *Ptent, double omega,
+                        nspb_csr_out *P, const nspb_opts *opts);
+/* Galerkin coarse operator A_c = R (A P) with R = P^T (returned in R when
+ * non-NULL). fp64.                                                           */
+int nspb_galerkin(const nspb_csr_in *A, const nspb_csr_in *P, nspb_csr_out *R,
+                  nspb_csr_out *Ac, const nspb_opts *opts);
+
 /* ---- seeded input generators (host memory) --------------------------------- */
 /* Each fills rowptr[nrows+1] and returns nnz (>=0) or a negative status; col
  * and val are filled when non-NULL. Values depend only on (seed, row, slot),

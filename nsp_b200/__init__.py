@@ -20,7 +20,7 @@ from .csr import DeviceCSR, HostCSR, adopt
 
 __all__ = ["spgemm", "spgemm_symbolic", "spgemm_numeric", "intprod", "nsp_spgemm_kernel_hash",
            "nsparseMGPU_version1", "DeviceCSR", "HostCSR", "gen", "NspbError", "lib",
-           "make_opts", "stats_dict", "matio"]
+           "make_opts", "stats_dict", "matio", "transpose", "sa_prolongator", "galerkin"]
 
 
 def _stream_ptr(stream):
@@ -75,6 +75,41 @@ def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR |
         res = DeviceCSR(A.nrows, B.ncols, adopt(c.rowptr, A.nrows + 1, "int32"),
                         adopt(c.col, c.nnz, "int32"), adopt(c.val, c.nnz, "float64"))
     return (res, stats_dict(st)) if return_stats else res
+
+
+def _adopt_out(c: CsrOut, vdtype="float64") -> DeviceCSR:
+    return DeviceCSR(c.nrows, c.ncols, adopt(c.rowptr, c.nrows + 1, "int32"),
+                     adopt(c.col, c.nnz, "int32"), adopt(c.val, c.nnz, vdtype))
+
+
+def transpose(A: DeviceCSR, stream=None) -> DeviceCSR:
+    """A^T through nspb_transpose (rows of the result list A's rows ascending;
+    the reference's CSRm::T, src/CSR.cu:738-785)."""
+    import torch
+    o = make_opts(stream=stream)
+    a, t = A.as_in(), CsrOut()
+    check(lib.nspb_transpose(C.byref(a), C.byref(t), C.byref(o)), "nspb_transpose")
+    return _adopt_out(t, "float32" if A.val.dtype == torch.float32 else "float64")
+
+
+def sa_prolongator(A: DeviceCSR, Ptent: DeviceCSR, omega: float = 2.0 / 3.0,
+                   stream=None) -> DeviceCSR:
+    """P = P_tent - omega D^-1 (A P_tent) through nspb_sa_prolongator."""
+    o = make_opts(stream=stream)
+    a, t, p = A.as_in(), Ptent.as_in(), CsrOut()
+    check(lib.nspb_sa_prolongator(C.byref(a), C.byref(t), C.c_double(omega), C.byref(p),
+                                  C.byref(o)), "nspb_sa_prolongator")
+    return _adopt_out(p)
+
+
+def galerkin(A: DeviceCSR, P: DeviceCSR, return_R: bool = False, stream=None):
+    """A_c = R (A P) with R = P^T through nspb_galerkin; (A_c, R) with return_R."""
+    o = make_opts(stream=stream)
+    a, p, r, ac = A.as_in(), P.as_in(), CsrOut(), CsrOut()
+    check(lib.nspb_galerkin(C.byref(a), C.byref(p), C.byref(r) if return_R else None,
+                            C.byref(ac), C.byref(o)), "nspb_galerkin")
+    Ac = _adopt_out(ac)
+    return (Ac, _adopt_out(r)) if return_R else Ac
 
 
 def spgemm_batched(As, Bs, precision: str = "fp64", stream=None, return_stats: bool = False):

@@ -118,6 +118,9 @@ _SIGS = {
                                     C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nspb_powerlaw_xmin": (C.c_double, [C.c_double, C.c_double, C.c_int32]),
     "nspb_nsp_spgemm_kernel_hash": (C.c_int, [P(SfCSR), P(SfCSR), P(SfCSR)]),
+    "nspb_transpose": (C.c_int, [P(CsrIn), P(CsrOut), P(Opts)]),
+    "nspb_sa_prolongator": (C.c_int, [P(CsrIn), P(CsrIn), C.c_double, P(CsrOut), P(Opts)]),
+    "nspb_galerkin": (C.c_int, [P(CsrIn), P(CsrIn), P(CsrOut), P(CsrOut), P(Opts)]),
     "nspb_read_coo_bin": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(HostCsr)]),
     "nspb_read_coo_ascii": (C.c_int, [C.c_char_p, P(HostCsr)]),
     "nspb_host_csr_free": (None, [P(HostCsr)]),

@@ -3,33 +3,20 @@
 The reference comes from an AMG solver whose setup forms the coarse
 operators R·A·P with its SpGEMM (the Galerkin products the MPI product of
 src/spspmpi.cu serves). This module builds that hierarchy on one GPU with
-this library's product:
+this library's device entry points:
 
   level l: A_l (n_l x n_l), aggregates of 3x3x3 nodes (the last aggregate of
   a dimension is ragged when the edge is not a multiple of 3),
-  P_tent(i, agg(i)) = 1, P = (I - w D^-1 A) P_tent with w = 2/3, R = P^T,
-  A_{l+1} = R (A P).
-
-Transposes and the smoothing update run on the host (setup code, not the
-measured path); the products A·P_tent, A·P and R·(AP) run through nspb.
+  P_tent(i, agg(i)) = 1                       (host: the aggregation map)
+  P = (I - w D^-1 A) P_tent, w = 2/3          nspb_sa_prolongator
+  R = P^T                                     nspb_transpose
+  A_{l+1} = R (A P)                           two nspb_spgemm products
 """
 from __future__ import annotations
 
 import numpy as np
 
 from .csr import HostCSR
-
-
-def _transpose(M: HostCSR) -> HostCSR:
-    """CSR transpose with columns ascending in every row (stable by row)."""
-    rows = np.repeat(np.arange(M.nrows, dtype=np.int64), np.diff(M.rowptr))
-    order = np.argsort(M.col, kind="stable")
-    tcol = rows[order].astype(np.int32)
-    tval = M.val[order]
-    counts = np.bincount(M.col, minlength=M.ncols)
-    trp = np.zeros(M.ncols + 1, dtype=np.int64)
-    np.cumsum(counts, out=trp[1:])
-    return HostCSR(M.ncols, M.nrows, trp.astype(np.int32), tcol, tval)
 
 
 def _tentative(nx: int, ny: int, nz: int, agg: int = 3):
@@ -43,39 +30,22 @@ def _tentative(nx: int, ny: int, nz: int, agg: int = 3):
     return P, (cx, cy, cz)
 
 
-def _product(A: HostCSR, B: HostCSR) -> HostCSR:
-    from . import spgemm
-    return spgemm(A.to_device(), B.to_device()).to_host()
-
-
-def smoothed_prolongator(A: HostCSR, Ptent: HostCSR, omega: float = 2.0 / 3.0) -> HostCSR:
-    """P = P_tent - omega D^-1 (A P_tent). The pattern of A·P_tent contains
-    agg(i) in row i (a_ii != 0), so P shares that pattern."""
-    AP = _product(A, Ptent)
-    rows = np.repeat(np.arange(A.nrows), np.diff(A.rowptr))
-    diag = np.zeros(A.nrows)
-    on = A.col == rows
-    diag[rows[on]] = A.val[on]
-    prow = np.repeat(np.arange(AP.nrows), np.diff(AP.rowptr))
-    val = -omega * AP.val / diag[prow]
-    tent = Ptent.col[prow] == AP.col
-    val[tent] += 1.0
-    return HostCSR(AP.nrows, AP.ncols, AP.rowptr, AP.col, val)
-
-
 def hierarchy(A0: HostCSR, grid, levels: int = 4, omega: float = 2.0 / 3.0):
-    """[(A_l, P_l, R_l, AP_l)] for l = 0 .. levels-2, and the coarsest A."""
+    """[(A_l, P_l, R_l, AP_l)] for l = 0 .. levels-2 (host copies), and the
+    coarsest A. Every operator is formed on the GPU."""
+    from . import sa_prolongator, spgemm, transpose
     out = []
-    A, (nx, ny, nz) = A0, grid
+    nx, ny, nz = grid
+    dA = A0.to_device()
     for _ in range(levels - 1):
         Pt, (nx, ny, nz) = _tentative(nx, ny, nz)
-        P = smoothed_prolongator(A, Pt, omega)
-        R = _transpose(P)
-        AP = _product(A, P)
-        Ac = _product(R, AP)
-        out.append((A, P, R, AP))
-        A = Ac
-    return out, A
+        dP = sa_prolongator(dA, Pt.to_device(), omega)
+        dR = transpose(dP)
+        dAP = spgemm(dA, dP)
+        dAc = spgemm(dR, dAP)
+        out.append((dA.to_host(), dP.to_host(), dR.to_host(), dAP.to_host()))
+        dA = dAc
+    return out, dA.to_host()
 
 
 def amg_batch(L: int = 96, levels: int = 4, seed: int = 20261203):
