@@ -101,7 +101,9 @@ typedef struct {
                             error words                                      */
   int32_t group_lanes;   /* 0 = auto; else 8, 16 or 32 lanes per row group    */
   int32_t timing;        /* 1: record CUDA events around each phase (stats)  */
-  int32_t _pad;
+  int32_t batch_max_products; /* batched calls and plans: at most this many
+                            products per block-diagonal group (0 = no limit
+                            beyond the int32 and size-based grouping)        */
   double comp_tol;       /* FP32_COMP: bound on |c - c*| / sum|a*b| per entry;
                             rows whose a-priori Dot2 bound exceeds it are
                             accumulated in fp64 (default 1e-10)              */
@@ -182,6 +184,25 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip,
 int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
                         nspb_stats *stats, void **owners, int32_t *n_owners);
+
+/* ---- plans: repeated products of a fixed structure --------------------------
+ * An AMG setup or a time loop often forms the same products again with new
+ * values. nspb_plan_create runs the symbolic phase of `count` products once
+ * (as one block-diagonal product when count > 1), allocates every C, runs
+ * one numeric pass and captures the numeric phase (counter reset, value
+ * concatenation, per-bin kernels, split) in a CUDA graph.
+ * nspb_plan_execute replays that graph on `stream`: it reads the CURRENT
+ * values behind A[p].val and B[p].val (same pointers, same structure as at
+ * creation) and rewrites C's values. C[p] point into plan-owned arrays that
+ * stay valid until nspb_plan_destroy. One plan must not be executed on two
+ * streams at once. opts.check_errors makes execute synchronise and report the
+ * device error word. fp64 or the fp32 compensated mode.                   */
+typedef struct nspb_plan_s *nspb_plan;
+int nspb_plan_create(int count, const nspb_csr_in *A, const nspb_csr_in *B,
+                     nspb_csr_out *C, const nspb_opts *opts, nspb_stats *stats,
+                     nspb_plan *plan);
+int nspb_plan_execute(nspb_plan plan, void *stream);
+int nspb_plan_destroy(nspb_plan plan);
 
 /* ---- column remap (compactcol / getmct) ------------------------------------ */
 /* Sorted unique column indices of col[0..nnz) that fall outside [first,last]

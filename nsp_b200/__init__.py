@@ -20,7 +20,7 @@ from .csr import DeviceCSR, HostCSR, adopt
 
 __all__ = ["spgemm", "spgemm_symbolic", "spgemm_numeric", "intprod", "nsp_spgemm_kernel_hash",
            "nsparseMGPU_version1", "DeviceCSR", "HostCSR", "gen", "NspbError", "lib",
-           "make_opts", "stats_dict", "matio", "transpose", "sa_prolongator", "galerkin"]
+           "make_opts", "stats_dict", "matio", "transpose", "sa_prolongator", "galerkin", "Plan"]
 
 
 def _stream_ptr(stream):
@@ -112,7 +112,59 @@ def galerkin(A: DeviceCSR, P: DeviceCSR, return_R: bool = False, stream=None):
     return (Ac, _adopt_out(r)) if return_R else Ac
 
 
-def spgemm_batched(As, Bs, precision: str = "fp64", stream=None, return_stats: bool = False):
+class _PlanView:
+    """Non-owning view of a plan-owned device array; keeps the plan alive."""
+
+    def __init__(self, plan, ptr: int, count: int, typestr: str):
+        self.plan, self.ptr, self.count, self.typestr = plan, int(ptr or 0), int(count), typestr
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": (self.count,), "typestr": self.typestr,
+                "data": (self.ptr, False), "version": 2, "strides": None}
+
+
+class Plan:
+    """Products of a fixed structure formed again and again (nspb_plan_*):
+    the symbolic phase and C's allocation happen once, execute() replays the
+    numeric phase from a CUDA graph with the current values of the inputs.
+    `C[p]` are DeviceCSR views of the plan's arrays."""
+
+    def __init__(self, As, Bs, precision: str = "fp64", check_errors: bool = True, stream=None,
+                 max_group: int = 0):
+        import torch
+        m = len(As)
+        prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+        o = make_opts(prec, False, check_errors, 0, 1e-10, stream)
+        o.batch_max_products = int(max_group)
+        a = (CsrIn * m)(*[x.as_in() for x in As])
+        b = (CsrIn * m)(*[x.as_in() for x in Bs])
+        c = (CsrOut * m)()
+        st = Stats()
+        h = C.c_void_p()
+        check(lib.nspb_plan_create(m, a, b, c, C.byref(o), C.byref(st), C.byref(h)),
+              "nspb_plan_create")
+        self._h = h
+        self._inputs = (list(As), list(Bs))  # the graph reads their arrays
+        self.stats = stats_dict(st)
+
+        def view(ptr, cnt, ts, dt):
+            return torch.as_tensor(_PlanView(self, ptr, cnt, ts), device="cuda").view(dt)
+        self.C = [DeviceCSR(c[p].nrows, c[p].ncols, view(c[p].rowptr, c[p].nrows + 1, "<i4", torch.int32),
+                            view(c[p].col, c[p].nnz, "<i4", torch.int32),
+                            view(c[p].val, c[p].nnz, "<f8", torch.float64)) for p in range(m)]
+
+    def execute(self, stream=None) -> None:
+        check(lib.nspb_plan_execute(self._h, _stream_ptr(stream)), "nspb_plan_execute")
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.nspb_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+
+def spgemm_batched(As, Bs, precision: str = "fp64", stream=None, return_stats: bool = False,
+                   max_group: int = 0):
     """C[p] = A[p]·B[p] for every pair through nspb_spgemm_batched (one
     block-diagonal product per group of products). Returns DeviceCSRs whose
     tensors view the shared output allocations (freed with the last view)."""
@@ -120,6 +172,7 @@ def spgemm_batched(As, Bs, precision: str = "fp64", stream=None, return_stats: b
     m = len(As)
     prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
     o = make_opts(prec, False, True, 0, 1e-10, stream)
+    o.batch_max_products = int(max_group)
     a = (CsrIn * m)(*[x.as_in() for x in As])
     b = (CsrIn * m)(*[x.as_in() for x in Bs])
     c = (CsrOut * m)()

@@ -52,7 +52,7 @@ class CsrOut(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("assume_sorted", C.c_int32),
                 ("check_errors", C.c_int32), ("group_lanes", C.c_int32),
-                ("timing", C.c_int32), ("_pad", C.c_int32),
+                ("timing", C.c_int32), ("batch_max_products", C.c_int32),
                 ("comp_tol", C.c_double), ("stream", C.c_void_p)]
 
 
@@ -118,6 +118,10 @@ _SIGS = {
                                     C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nspb_powerlaw_xmin": (C.c_double, [C.c_double, C.c_double, C.c_int32]),
     "nspb_nsp_spgemm_kernel_hash": (C.c_int, [P(SfCSR), P(SfCSR), P(SfCSR)]),
+    "nspb_plan_create": (C.c_int, [C.c_int, P(CsrIn), P(CsrIn), P(CsrOut), P(Opts), P(Stats),
+                                   P(C.c_void_p)]),
+    "nspb_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nspb_plan_destroy": (C.c_int, [C.c_void_p]),
     "nspb_transpose": (C.c_int, [P(CsrIn), P(CsrOut), P(Opts)]),
     "nspb_sa_prolongator": (C.c_int, [P(CsrIn), P(CsrIn), C.c_double, P(CsrOut), P(Opts)]),
     "nspb_galerkin": (C.c_int, [P(CsrIn), P(CsrIn), P(CsrOut), P(CsrOut), P(Opts)]),

@@ -150,7 +150,7 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   return NSPB_OK;
 }
 
-int Call::alloc_scratch() {
+size_t Call::scratch_bytes() {
   const size_t nn = (size_t)std::max(n, 1);
   off_row_nz = 0;
   off_perm = align256(off_row_nz + (nn + 1) * 4);
@@ -158,6 +158,11 @@ int Call::alloc_scratch() {
   off_tiles = align256(off_counters + sizeof(DevCounters));
   const size_t tiles = (size_t)scan_tiles(n);
   ws_bytes = align256(off_tiles + tiles * 8);
+  return ws_bytes;
+}
+
+int Call::alloc_scratch() {
+  scratch_bytes();
   if (ext_ws) {
     if (ws_bytes > ext_bytes) return NSPB_ERR_CAPACITY;
     ws = ext_ws;

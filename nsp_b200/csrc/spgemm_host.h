@@ -72,6 +72,7 @@ struct Call {
   }
 
   int init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o);
+  size_t scratch_bytes();  // sets the scratch offsets; bytes alloc_scratch needs
   int alloc_scratch();
   int cuda_fail(cudaError_t e);
   int fetch_counters();
