@@ -108,6 +108,10 @@ typedef struct {
                             rows whose a-priori Dot2 bound exceeds it are
                             accumulated in fp64 (default 1e-10)              */
   void *stream;          /* cudaStream_t                                     */
+  int32_t num_table_shift; /* 0: numeric row-group tables of twice the bin's
+                            entry limit (load <= 1/2); 1: four times (load
+                            <= 1/4); chosen by nspb_autotune              */
+  int32_t _reserved;
 } nspb_opts;
 
 /* Per-call figures (all optional; pass NULL).                               */
@@ -184,6 +188,22 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip,
 int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
                         nspb_stats *stats, void **owners, int32_t *n_owners);
+
+/* ---- autotuner ---------------------------------------------------------------
+ * Times this product (C sized once, then written into the same arrays) with
+ * every candidate of threads per row (group_lanes 8, 16, 32) and numeric
+ * table size (num_table_shift 0, 1): one warm-up and `reps` timed calls each,
+ * CUDA events on opts->stream. *best receives `base` with the fastest
+ * candidate's knobs; report (may be NULL; room for 6) the candidates and
+ * their mean ms, *n_report their number.                                   */
+typedef struct {
+  int32_t group_lanes;
+  int32_t num_table_shift;
+  float ms;
+  int32_t _pad;
+} nspb_tune_entry;
+int nspb_autotune(const nspb_csr_in *A, const nspb_csr_in *B, const nspb_opts *base,
+                  int reps, nspb_opts *best, nspb_tune_entry *report, int32_t *n_report);
 
 /* ---- plans: repeated products of a fixed structure --------------------------
  * An AMG setup or a time loop often forms the same products again with new

@@ -20,7 +20,8 @@ from .csr import DeviceCSR, HostCSR, adopt
 
 __all__ = ["spgemm", "spgemm_symbolic", "spgemm_numeric", "intprod", "nsp_spgemm_kernel_hash",
            "nsparseMGPU_version1", "DeviceCSR", "HostCSR", "gen", "NspbError", "lib",
-           "make_opts", "stats_dict", "matio", "transpose", "sa_prolongator", "galerkin", "Plan"]
+           "make_opts", "stats_dict", "matio", "transpose", "sa_prolongator", "galerkin", "Plan",
+           "autotune"]
 
 
 def _stream_ptr(stream):
@@ -31,7 +32,7 @@ def _stream_ptr(stream):
 
 
 def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group_lanes=0,
-              comp_tol=1e-10, stream=None) -> Opts:
+              comp_tol=1e-10, stream=None, table_shift=0) -> Opts:
     o = Opts()
     lib.nspb_default_opts(C.byref(o))
     o.precision = precision
@@ -40,6 +41,7 @@ def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group
     o.group_lanes = int(group_lanes)
     o.comp_tol = float(comp_tol)
     o.stream = _stream_ptr(stream)
+    o.num_table_shift = int(table_shift)
     return o
 
 
@@ -51,14 +53,15 @@ def stats_dict(s: Stats) -> dict:
 
 def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,
            stream=None, check_errors: bool = True, assume_sorted: bool = False,
-           group_lanes: int = 0, comp_tol: float = 1e-10, return_stats: bool = False):
+           group_lanes: int = 0, comp_tol: float = 1e-10, return_stats: bool = False,
+           table_shift: int = 0):
     """C = A·B on the current CUDA device through nspb_spgemm.
 
     With `out` given, its tensors are used as C's arrays (capacity = their
     length); otherwise the library allocates C (freed with the tensors)."""
     import torch
     prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
-    o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream)
+    o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream, table_shift)
     a, b = A.as_in(), B.as_in()
     c = CsrOut()
     if out is not None:
@@ -110,6 +113,22 @@ def galerkin(A: DeviceCSR, P: DeviceCSR, return_R: bool = False, stream=None):
                             C.byref(ac), C.byref(o)), "nspb_galerkin")
     Ac = _adopt_out(ac)
     return (Ac, _adopt_out(r)) if return_R else Ac
+
+
+def autotune(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", reps: int = 3, stream=None):
+    """nspb_autotune: ({"group_lanes", "table_shift"} of the fastest candidate,
+    [(group_lanes, table_shift, ms), ...] for every candidate)."""
+    from ._lib import TuneEntry
+    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    o = make_opts(prec, stream=stream)
+    best = Opts()
+    rep = (TuneEntry * 6)()
+    n = C.c_int32(0)
+    a, b = A.as_in(), B.as_in()
+    check(lib.nspb_autotune(C.byref(a), C.byref(b), C.byref(o), int(reps), C.byref(best), rep,
+                            C.byref(n)), "nspb_autotune")
+    return ({"group_lanes": best.group_lanes, "table_shift": best.num_table_shift},
+            [(rep[i].group_lanes, rep[i].num_table_shift, rep[i].ms) for i in range(n.value)])
 
 
 class _PlanView:

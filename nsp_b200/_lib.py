@@ -53,7 +53,8 @@ class Opts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("assume_sorted", C.c_int32),
                 ("check_errors", C.c_int32), ("group_lanes", C.c_int32),
                 ("timing", C.c_int32), ("batch_max_products", C.c_int32),
-                ("comp_tol", C.c_double), ("stream", C.c_void_p)]
+                ("comp_tol", C.c_double), ("stream", C.c_void_p),
+                ("num_table_shift", C.c_int32), ("_reserved", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -63,6 +64,11 @@ class Stats(C.Structure):
                 ("max_row_err", C.c_double), ("launches", C.c_int32),
                 ("ms_rowinfo", C.c_float), ("ms_symbolic", C.c_float),
                 ("ms_scan", C.c_float), ("ms_numeric", C.c_float), ("_pad", C.c_float)]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("group_lanes", C.c_int32), ("num_table_shift", C.c_int32),
+                ("ms", C.c_float), ("_pad", C.c_int32)]
 
 
 class HostCsr(C.Structure):
@@ -122,6 +128,8 @@ _SIGS = {
                                    P(C.c_void_p)]),
     "nspb_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nspb_plan_destroy": (C.c_int, [C.c_void_p]),
+    "nspb_autotune": (C.c_int, [P(CsrIn), P(CsrIn), P(Opts), C.c_int, P(Opts), P(TuneEntry),
+                                P(C.c_int32)]),
     "nspb_transpose": (C.c_int, [P(CsrIn), P(CsrOut), P(Opts)]),
     "nspb_sa_prolongator": (C.c_int, [P(CsrIn), P(CsrIn), C.c_double, P(CsrOut), P(Opts)]),
     "nspb_galerkin": (C.c_int, [P(CsrIn), P(CsrIn), P(CsrOut), P(CsrOut), P(Opts)]),

@@ -66,13 +66,14 @@ cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const CsrDev 
 
 // ---- numeric.cu -----------------------------------------------------------------
 // owned: B rows hold no duplicate columns (deterministic plain accumulation).
+// tshift: the row-group bins use tables 2^tshift times their default size.
 // b_sorted: B rows strictly increasing (long rows take their column span
 // from the ends of the B rows they touch).
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
                                const CsrDev &A, const CsrDev &B,
                                const int *crpt, int *ccol, double *cval,
                                const int *rows, int count, int *err, int *ticket,
-                               cudaStream_t s);
+                               int tshift, cudaStream_t s);
 
 // Compensated numeric step (fp32 inputs): rows with at most nmax A entries
 // accumulate error-free fp32 pairs (TwoProduct + TwoSum) collapsed to fp64;
@@ -83,6 +84,6 @@ cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorte
                                     const CsrDev &A, const CsrDev &B, const int *crpt,
                                     int *ccol, double *cval, const int *rows, int count,
                                     int nmax, int *redo, int *max_deg, int *err,
-                                    int *ticket, cudaStream_t s);
+                                    int *ticket, int tshift, cudaStream_t s);
 
 }  // namespace nspb

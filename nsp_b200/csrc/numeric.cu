@@ -574,15 +574,17 @@ template <int G, bool OWNED, typename VT, bool COMP>
 static cudaError_t num_group_bin(int bin, const CsrDev &A, const CsrDev &B, const VT *av,
                                  const VT *bv, const int *crpt, int *ccol, double *cval,
                                  const int *rows, int count, int *err, CompArgs comp,
-                                 cudaStream_t s) {
+                                 int tshift, cudaStream_t s) {
 #define NSPB_NG(L2T) \
   run_num_group<G, L2T, OWNED, VT, COMP>(A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
-  switch (bin) {
-    case 0: return NSPB_NG(5);
-    case 1: return NSPB_NG(6);
-    case 2: return NSPB_NG(7);
-    case 3: return NSPB_NG(8);
-    case 4: return NSPB_NG(9);
+  // bin b holds rows of at most 16 << b entries; its table has 32 << (b + tshift)
+  // slots (load <= 1/2 or 1/4), 1024 at most
+  switch (std::min(5 + bin + tshift, 10)) {
+    case 5: return NSPB_NG(5);
+    case 6: return NSPB_NG(6);
+    case 7: return NSPB_NG(7);
+    case 8: return NSPB_NG(8);
+    case 9: return NSPB_NG(9);
     default: return NSPB_NG(10);
   }
 #undef NSPB_NG
@@ -606,10 +608,11 @@ template <typename VT, bool COMP>
 static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, const CsrDev &A,
                                  const CsrDev &B, const VT *av, const VT *bv, const int *crpt,
                                  int *ccol, double *cval, const int *rows, int count, int *err,
-                                 CompArgs comp, int *ticket, cudaStream_t s) {
+                                 CompArgs comp, int *ticket, int tshift, cudaStream_t s) {
   if (bin < kNumGroupBins) {
 #define NSPB_GB(GL, OW) \
-  num_group_bin<GL, OW, VT, COMP>(bin, A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
+  num_group_bin<GL, OW, VT, COMP>(bin, A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, \
+                                  tshift, s)
     if (owned) {
       if (lanes == 8) return NSPB_GB(8, true);
       if (lanes == 16) return NSPB_GB(16, true);
@@ -640,22 +643,22 @@ static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, 
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
                                const CsrDev &A, const CsrDev &B, const int *crpt,
                                int *ccol, double *cval, const int *rows, int count,
-                               int *err, int *ticket, cudaStream_t s) {
+                               int *err, int *ticket, int tshift, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   return numeric_bin_t<double, false>(bin, lanes, owned, b_sorted, A, B, A.val, B.val, crpt,
                                       ccol, cval, rows, count, err, CompArgs{0, nullptr, nullptr},
-                                      ticket, s);
+                                      ticket, tshift, s);
 }
 
 cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorted,
                                     const CsrDev &A, const CsrDev &B, const int *crpt,
                                     int *ccol, double *cval, const int *rows, int count,
                                     int nmax, int *redo, int *max_deg, int *err,
-                                    int *ticket, cudaStream_t s) {
+                                    int *ticket, int tshift, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   return numeric_bin_t<float, true>(bin, lanes, owned, b_sorted, A, B, A.val32, B.val32, crpt,
                                     ccol, cval, rows, count, err, CompArgs{nmax, redo, max_deg},
-                                    ticket, s);
+                                    ticket, tshift, s);
 }
 
 }  // namespace nspb

@@ -294,11 +294,12 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
     int *ticket = &ctr->ticket[16 + b];
+    const int tshift = opts.num_table_shift == 1 ? 1 : 0;
     e = comp ? launch_numeric_comp_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows,
                                        c, nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err,
-                                       ticket, s)
+                                       ticket, tshift, s)
              : launch_numeric_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows, c,
-                                  &ctr->err, ticket, s);
+                                  &ctr->err, ticket, tshift, s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
