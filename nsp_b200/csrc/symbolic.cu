@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// ---- rows of 6K intermediate products and more: one block per row -------------
+// ---- rows of more than 3072 intermediate products: one block per row ---------
 // Distinct columns are counted as set bits of a shared-memory bitmap over the
 // row's column span [lo, hi] (see row_span), in windows of 2^20 columns. A
 // row whose span is wider than one window but whose products fit a 2^15-slot
