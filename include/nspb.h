@@ -189,6 +189,20 @@ int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
                         nspb_stats *stats, void **owners, int32_t *n_owners);
 
+/* ---- host-memory operands --------------------------------------------------
+ * C = A·B with A, B (nspb_csr_in whose pointers are HOST memory, row pointers
+ * starting at 0) and C in host memory. Structure is copied first, values on
+ * a second stream while the symbolic phase runs; the numeric phase runs in
+ * `nblocks` row blocks (0 = 8) whose columns and values are copied back while
+ * the next block is computed. Pinned host arrays give full-bandwidth,
+ * overlapped copies. h_rowptr receives n+1 entries; h_col/h_val must hold
+ * h_capacity entries: with fewer than nnz(C) (or NULL) only the row pointer
+ * is written, *nnz_out tells the size and NSPB_ERR_CAPACITY is returned.
+ * When B's three host arrays are A's, they are copied once.             */
+int nspb_spgemm_host(const nspb_csr_in *hA, const nspb_csr_in *hB, int32_t *h_rowptr,
+                     int32_t *h_col, double *h_val, int64_t h_capacity, int64_t *nnz_out,
+                     int32_t nblocks, const nspb_opts *opts);
+
 /* ---- autotuner ---------------------------------------------------------------
  * Times this product (C sized once, then written into the same arrays) with
  * every candidate of threads per row (group_lanes 8, 16, 32) and numeric

@@ -21,7 +21,7 @@ from .csr import DeviceCSR, HostCSR, adopt
 __all__ = ["spgemm", "spgemm_symbolic", "spgemm_numeric", "intprod", "nsp_spgemm_kernel_hash",
            "nsparseMGPU_version1", "DeviceCSR", "HostCSR", "gen", "NspbError", "lib",
            "make_opts", "stats_dict", "matio", "transpose", "sa_prolongator", "galerkin", "Plan",
-           "autotune"]
+           "autotune", "spgemm_host"]
 
 
 def _stream_ptr(stream):
@@ -129,6 +129,46 @@ def autotune(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", reps: int = 3,
                             C.byref(n)), "nspb_autotune")
     return ({"group_lanes": best.group_lanes, "table_shift": best.num_table_shift},
             [(rep[i].group_lanes, rep[i].num_table_shift, rep[i].ms) for i in range(n.value)])
+
+
+def _host_ptr(x):
+    import numpy as np
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()  # CPU (pinned) torch tensor
+
+
+def spgemm_host(A, B, out=None, nblocks: int = 0, precision: str = "fp64", stream=None):
+    """C = A·B with host operands through nspb_spgemm_host. A and B expose
+    nrows, ncols and host arrays rowptr/col/val (numpy, or CPU torch tensors,
+    pinned for overlapped copies). With `out` = (rowptr, col, val) host arrays
+    of enough capacity C is written there; otherwise numpy arrays are sized by
+    a first call. Returns (rowptr, col, val)."""
+    import numpy as np
+    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    o = make_opts(prec, stream=stream)
+
+    def host_in(M):
+        d = CsrIn()
+        d.nrows, d.ncols = M.nrows, M.ncols
+        d.nnz = int(M.rowptr[M.nrows])
+        d.rowptr, d.col, d.val = _host_ptr(M.rowptr), _host_ptr(M.col), _host_ptr(M.val)
+        d.val_type = F32 if str(M.val.dtype).endswith("float32") else F64
+        return d
+    a, b = host_in(A), host_in(B)
+    nnz = C.c_int64(0)
+    if out is None:
+        rp = np.empty(A.nrows + 1, np.int32)
+        st = lib.nspb_spgemm_host(C.byref(a), C.byref(b), rp.ctypes.data, None, None, 0,
+                                  C.byref(nnz), int(nblocks), C.byref(o))
+        if st not in (0, -8):
+            check(st, "nspb_spgemm_host")
+        out = (rp, np.empty(max(nnz.value, 1), np.int32), np.empty(max(nnz.value, 1), np.float64))
+    rp, col, val = out
+    cap = min(len(col), len(val))
+    check(lib.nspb_spgemm_host(C.byref(a), C.byref(b), _host_ptr(rp), _host_ptr(col), _host_ptr(val),
+                               cap, C.byref(nnz), int(nblocks), C.byref(o)), "nspb_spgemm_host")
+    return rp, col[:nnz.value], val[:nnz.value]
 
 
 class _PlanView:

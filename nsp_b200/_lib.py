@@ -130,6 +130,8 @@ _SIGS = {
     "nspb_plan_destroy": (C.c_int, [C.c_void_p]),
     "nspb_autotune": (C.c_int, [P(CsrIn), P(CsrIn), P(Opts), C.c_int, P(Opts), P(TuneEntry),
                                 P(C.c_int32)]),
+    "nspb_spgemm_host": (C.c_int, [P(CsrIn), P(CsrIn), C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int64, P(C.c_int64), C.c_int32, P(Opts)]),
     "nspb_transpose": (C.c_int, [P(CsrIn), P(CsrOut), P(Opts)]),
     "nspb_sa_prolongator": (C.c_int, [P(CsrIn), P(CsrIn), C.c_double, P(CsrOut), P(Opts)]),
     "nspb_galerkin": (C.c_int, [P(CsrIn), P(CsrIn), P(CsrOut), P(CsrOut), P(Opts)]),

@@ -1,0 +1,228 @@
+// C = A·B with A, B and C in host memory: the copies overlap the product.
+//
+// The reference's caller copies its matrices to the device, calls the product
+// and copies C back, one step after the other (src/CSR.cu:656-683 copyToDevice
+// / copyToHost around nsparseMGPU). Here, on two streams:
+//   1. A's and B's row pointers and columns go to the device first; their
+//      values follow on the copy stream while the symbolic phase runs (it
+//      needs no values);
+//   2. C's row pointer comes back and cuts the rows into blocks of about
+//      equal nnz;
+//   3. each block's numeric step runs on the compute stream into one of two
+//      device buffers, whose columns and values are copied to the caller's
+//      host arrays on the copy stream while the next block is computed.
+// With pinned host arrays the D2H copy of C, the largest transfer, runs under
+// the numeric phase.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+#include "spgemm_host.h"
+
+namespace nspb {
+
+__global__ void k_rebase_slice(const int *__restrict__ in, int first, int n, int *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
+    out[i] = in[first + i] - in[first];
+}
+
+namespace {
+
+struct Pool {
+  cudaStream_t s;
+  std::vector<void *> blocks;
+  explicit Pool(cudaStream_t st) : s(st) {}
+  ~Pool() {
+    for (void *p : blocks) scratch_free(p, s);
+  }
+  template <typename T>
+  int get(T **p, size_t count) {
+    void *q = nullptr;
+    const int st = scratch_alloc(&q, std::max<size_t>(count, 1) * sizeof(T), s);
+    if (st) return st;
+    blocks.push_back(q);
+    *p = static_cast<T *>(q);
+    return NSPB_OK;
+  }
+};
+
+struct Streams {
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev[6] = {};
+  ~Streams() {
+    if (copy) cudaStreamDestroy(copy);
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+int fail(cudaError_t e) {
+  g_last_cuda = (int)e;
+  cudaGetLastError();
+  return NSPB_ERR_CUDA;
+}
+
+bool valid_host(const nspb_csr_in *M) {
+  if (!M || M->nrows < 0 || M->ncols < 0 || M->nnz < 0 || M->nnz > INT32_MAX) return false;
+  if (!M->rowptr) return false;
+  if (M->nnz > 0 && (!M->col || !M->val)) return false;
+  return M->val_type == NSPB_F64 || M->val_type == NSPB_F32;
+}
+
+}  // namespace
+}  // namespace nspb
+
+using namespace nspb;
+
+extern "C" int nspb_spgemm_host(const nspb_csr_in *hA, const nspb_csr_in *hB, int32_t *h_rowptr,
+                                int32_t *h_col, double *h_val, int64_t h_capacity,
+                                int64_t *nnz_out, int32_t nblocks, const nspb_opts *opts) {
+  if (!valid_host(hA) || !valid_host(hB) || !h_rowptr || !nnz_out) return NSPB_ERR_INVALID;
+  if (hA->ncols != hB->nrows || hA->val_type != hB->val_type) return NSPB_ERR_INVALID;
+  if (hA->rowptr[0] != 0 || hB->rowptr[0] != 0 || hA->rowptr[hA->nrows] != hA->nnz ||
+      hB->rowptr[hB->nrows] != hB->nnz)
+    return NSPB_ERR_INVALID;
+  nspb_opts o;
+  nspb_default_opts(&o);
+  if (opts) o = *opts;
+  o.timing = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(o.stream);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return NSPB_ERR_NO_DEVICE;
+  }
+  const size_t vsz = hA->val_type == NSPB_F32 ? 4 : 8;
+  const bool same = hA->rowptr == hB->rowptr && hA->col == hB->col && hA->val == hB->val &&
+                    hA->nrows == hB->nrows && hA->nnz == hB->nnz;
+  const int n = hA->nrows;
+  Streams ss;
+  cudaError_t e = cudaStreamCreateWithFlags(&ss.copy, cudaStreamNonBlocking);
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i)
+    e = cudaEventCreateWithFlags(&ss.ev[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) return fail(e);
+  cudaEvent_t &ev_alloc = ss.ev[0], &ev_vals = ss.ev[1];
+  cudaEvent_t *computed = ss.ev + 2, *copied = ss.ev + 4;
+  Pool pool(s);
+  int st;
+  // 1. device operands: structure on the compute stream, values on the copy stream
+  int *arp = nullptr, *acl = nullptr, *brp = nullptr, *bcl = nullptr;
+  char *aval = nullptr, *bval = nullptr;
+  if ((st = pool.get(&arp, (size_t)n + 1)) || (st = pool.get(&acl, (size_t)hA->nnz)) ||
+      (st = pool.get(&aval, (size_t)hA->nnz * vsz)))
+    return st;
+  if (same) {
+    brp = arp;
+    bcl = acl;
+    bval = aval;
+  } else if ((st = pool.get(&brp, (size_t)hB->nrows + 1)) ||
+             (st = pool.get(&bcl, (size_t)hB->nnz)) ||
+             (st = pool.get(&bval, (size_t)hB->nnz * vsz))) {
+    return st;
+  }
+  auto h2d = [&](void *d, const void *h, size_t bytes, cudaStream_t st_) {
+    return bytes ? cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st_) : cudaSuccess;
+  };
+  e = h2d(arp, hA->rowptr, ((size_t)n + 1) * 4, s);
+  if (e == cudaSuccess) e = h2d(acl, hA->col, (size_t)hA->nnz * 4, s);
+  if (e == cudaSuccess && !same) e = h2d(brp, hB->rowptr, ((size_t)hB->nrows + 1) * 4, s);
+  if (e == cudaSuccess && !same) e = h2d(bcl, hB->col, (size_t)hB->nnz * 4, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ev_alloc, s);  // allocations ordered first
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ss.copy, ev_alloc, 0);
+  if (e == cudaSuccess) e = h2d(aval, hA->val, (size_t)hA->nnz * vsz, ss.copy);
+  if (e == cudaSuccess && !same) e = h2d(bval, hB->val, (size_t)hB->nnz * vsz, ss.copy);
+  if (e == cudaSuccess) e = cudaEventRecord(ev_vals, ss.copy);
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(ss.copy);
+    return fail(e);
+  }
+  const nspb_csr_in dA = {n, hA->ncols, hA->nnz, arp, acl, aval, hA->val_type, 0};
+  const nspb_csr_in dB = {hB->nrows, hB->ncols, hB->nnz, brp, bcl, bval, hB->val_type, 0};
+  // 2. symbolic phase (no values needed), C's row pointer to the host
+  int *crpt = nullptr;
+  if ((st = pool.get(&crpt, (size_t)n + 1))) {
+    cudaStreamSynchronize(ss.copy);
+    return st;
+  }
+  int64_t nnz = 0;
+  bool b_sorted = true;
+  {
+    Call sym;
+    if (!(st = sym.init(&dA, &dB, &o))) st = sym.symbolic(crpt, &nnz);
+    b_sorted = sym.b_sorted;
+  }
+  if (!st) {
+    e = cudaMemcpyAsync(h_rowptr, crpt, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = fail(e);
+  }
+  if (st) {
+    cudaStreamSynchronize(ss.copy);
+    return st;
+  }
+  *nnz_out = nnz;
+  if (!h_col || !h_val || h_capacity < nnz) {
+    cudaStreamSynchronize(ss.copy);
+    return nnz == 0 ? NSPB_OK : NSPB_ERR_CAPACITY;
+  }
+  if ((e = cudaStreamWaitEvent(s, ev_vals, 0)) != cudaSuccess) {
+    cudaStreamSynchronize(ss.copy);
+    return fail(e);
+  }
+  // 3. row blocks of about nnz/nb entries, two buffers in flight
+  const int nb = std::max(1, std::min(nblocks > 0 ? nblocks : 8, std::max(n, 1)));
+  std::vector<int> cut(1, 0);
+  for (int k = 1; k < nb; ++k) {
+    const long long target = nnz * k / nb;
+    const int r = (int)(std::lower_bound(h_rowptr, h_rowptr + n + 1, (int32_t)target) - h_rowptr);
+    if (r > cut.back() && r < n) cut.push_back(r);
+  }
+  cut.push_back(n);
+  long long max_rows = 0, max_nnz = 0;
+  for (size_t k = 0; k + 1 < cut.size(); ++k) {
+    max_rows = std::max<long long>(max_rows, cut[k + 1] - cut[k]);
+    max_nnz = std::max<long long>(max_nnz, (long long)h_rowptr[cut[k + 1]] - h_rowptr[cut[k]]);
+  }
+  int *bcrp[2] = {nullptr, nullptr}, *bcol[2] = {nullptr, nullptr};
+  double *bvl[2] = {nullptr, nullptr};
+  for (int b = 0; b < 2 && !st; ++b)
+    if ((st = pool.get(&bcrp[b], (size_t)max_rows + 1)) || (st = pool.get(&bcol[b], (size_t)max_nnz)) ||
+        (st = pool.get(&bvl[b], (size_t)max_nnz)))
+      break;
+  nspb_opts ob = o;
+  ob.assume_sorted = b_sorted ? 1 : 0;  // checked once by the symbolic phase
+  for (size_t k = 0; k + 1 < cut.size() && !st; ++k) {
+    const int b = (int)(k & 1);
+    const int r0 = cut[k], r1 = cut[k + 1], nr = r1 - r0;
+    const long long c0 = h_rowptr[r0], cnt = (long long)h_rowptr[r1] - c0;
+    if (k >= 2 && (e = cudaStreamWaitEvent(s, copied[b], 0)) != cudaSuccess) {
+      st = fail(e);
+      break;
+    }
+    k_rebase_slice<<<std::max(1, std::min((nr + 256) / 256, dev_info().sms * 8)), 256, 0, s>>>(
+        crpt, r0, nr, bcrp[b]);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+      st = fail(e);
+      break;
+    }
+    const nspb_csr_in Ab = {nr, hA->ncols, (int64_t)hA->rowptr[r1] - hA->rowptr[r0], arp + r0, acl,
+                            aval, hA->val_type, 0};
+    nspb_csr_out Cb = {nr, hB->ncols, cnt, bcrp[b], bcol[b], bvl[b], max_nnz};
+    if ((st = nspb_spgemm_numeric(&Ab, &dB, &Cb, &ob, nullptr))) break;
+    e = cudaEventRecord(computed[b], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ss.copy, computed[b], 0);
+    if (e == cudaSuccess && cnt > 0)
+      e = cudaMemcpyAsync(h_col + c0, bcol[b], (size_t)cnt * 4, cudaMemcpyDeviceToHost, ss.copy);
+    if (e == cudaSuccess && cnt > 0)
+      e = cudaMemcpyAsync(h_val + c0, bvl[b], (size_t)cnt * 8, cudaMemcpyDeviceToHost, ss.copy);
+    if (e == cudaSuccess) e = cudaEventRecord(copied[b], ss.copy);
+    if (e != cudaSuccess) st = fail(e);
+  }
+  e = cudaStreamSynchronize(ss.copy);
+  if (!st && e != cudaSuccess) st = fail(e);
+  e = cudaStreamSynchronize(s);
+  if (!st && e != cudaSuccess) st = fail(e);
+  return st;
+}

@@ -1,0 +1,73 @@
+"""nspb_spgemm_host: operands and result in host memory, copies overlapped
+with the row-blocked numeric phase; results against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import nsp_b200 as nb
+import oracle
+from nsp_b200._lib import ERR_CAPACITY
+from nsp_b200.csr import HostCSR
+
+from conftest import assert_bitwise, assert_close, assert_same_structure
+
+pytestmark = pytest.mark.gpu
+
+
+def check(res, A, B, exact=True):
+    rp, col, val = oracle.spgemm(A, B)
+    assert_same_structure(np.asarray(res[0]), np.asarray(res[1]), rp, col)
+    if exact:
+        assert_bitwise(np.asarray(res[2]), val)
+    else:
+        assert_close(np.asarray(res[2]), val, oracle.absbound(A, B, rp, col))
+
+
+class Pinned:
+    def __init__(self, M):
+        self.nrows, self.ncols = M.nrows, M.ncols
+        self.rowptr = torch.from_numpy(M.rowptr).pin_memory()
+        self.col = torch.from_numpy(M.col).pin_memory()
+        self.val = torch.from_numpy(M.val).pin_memory()
+
+
+@pytest.mark.parametrize("nblocks", [0, 1, 3, 64])
+def test_host_product_blocks(cuda, nblocks):
+    A = nb.gen.random(5000, 4000, 0, 30, seed=3)
+    B = nb.gen.random(4000, 3500, 0, 12, seed=4)
+    check(nb.spgemm_host(A, B, nblocks=nblocks), A, B)
+
+
+def test_host_pinned_and_aliased(cuda):
+    A = nb.gen.stencil(20, npts=27)
+    pA = Pinned(A)
+    n = A.nrows
+    _, st = nb.spgemm(A.to_device(), A.to_device(), return_stats=True)
+    out = (torch.empty(n + 1, dtype=torch.int32).pin_memory(),
+           torch.empty(st["nnz"], dtype=torch.int32).pin_memory(),
+           torch.empty(st["nnz"], dtype=torch.float64).pin_memory())
+    res = nb.spgemm_host(pA, pA, out=out, nblocks=5)  # B's arrays are A's: copied once
+    check(tuple(x.numpy() for x in res), A, A)
+
+
+def test_host_long_rows_and_unsorted(cuda):
+    P = nb.gen.powerlaw(30_000, max_deg=6000, seed=5)
+    check(nb.spgemm_host(P, P, nblocks=7), P, P, exact=False)
+    rng = np.random.default_rng(2)
+    col = P.col.copy()
+    for i in range(0, P.nrows, 4):
+        rng.shuffle(col[P.rowptr[i]:P.rowptr[i + 1]])
+    Pu = HostCSR(P.nrows, P.ncols, P.rowptr, col, P.val)
+    check(nb.spgemm_host(P, Pu, nblocks=4), P, Pu, exact=False)
+
+
+def test_host_capacity(cuda):
+    A = nb.gen.random(300, 200, 1, 8, seed=6)
+    B = nb.gen.random(200, 100, 1, 8, seed=7)
+    rp = np.empty(301, np.int32)
+    small = (rp, np.empty(5, np.int32), np.empty(5, np.float64))
+    with pytest.raises(nb.NspbError) as e:
+        nb.spgemm_host(A, B, out=small)
+    assert e.value.status == ERR_CAPACITY
+    want, _, _ = oracle.spgemm(A, B)
+    assert np.array_equal(rp, want)  # the row pointer is written even then
