@@ -68,3 +68,33 @@ def test_no_device_reports_status():
     c = _lib.CsrOut()
     st = nb.lib.nspb_spgemm(ctypes.byref(a), ctypes.byref(a), ctypes.byref(c), None, None)
     assert st == _lib.ERR_NO_DEVICE
+
+
+def test_header_is_plain_c_and_layouts_match(tmp_path):
+    """include/nspb.h compiles as C99 with warnings as errors, a C program
+    links libnspb.so, and the struct sizes it sees equal the Python
+    bindings' (no GPU call is made)."""
+    src = tmp_path / "abi.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "nspb.h"
+int main(void) {
+  nspb_opts o;
+  nspb_default_opts(&o);
+  printf("%zu %zu %zu %zu %zu %zu %zu %d %s\n", sizeof(nspb_csr_in), sizeof(nspb_csr_out),
+         sizeof(nspb_opts), sizeof(nspb_stats), sizeof(nspb_host_csr), sizeof(nspb_tune_entry),
+         sizeof(void *), o.precision, nspb_version());
+  return o.comp_tol > 0.0 ? 0 : 1;
+}
+''')
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run(["/usr/bin/gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                    "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lnspb", "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    sizes = [int(x) for x in out[:7]]
+    assert sizes == [ctypes.sizeof(_lib.CsrIn), ctypes.sizeof(_lib.CsrOut),
+                     ctypes.sizeof(_lib.Opts), ctypes.sizeof(_lib.Stats),
+                     ctypes.sizeof(_lib.HostCsr), ctypes.sizeof(_lib.TuneEntry), 8]
+    assert int(out[7]) == _lib.PREC_FP64
