@@ -58,6 +58,7 @@ __host__ __device__ __forceinline__ int num_bin(int nz) {
 }
 
 // ---- hashing --------------------------------------------------------------------
+
 // Fibonacci hashing: the HIGH bits of key*2^32/phi. Keys that differ by a
 // multiple of a power of two (stencil planes n^2 apart) still spread, and runs
 // of consecutive keys land on distinct shared-memory banks.
@@ -80,10 +81,16 @@ __device__ __forceinline__ double ld_stream(const double *p) {
   return v;
 }
 
+// Probe sequences: linear (QUAD false: h, h+1, h+2, ...), best for the
+// clustered columns of row groups; or triangular (QUAD true: h, h+1, h+3,
+// h+6, ...), which breaks up clusters in the larger tables of block-per-row
+// rows. Both visit every slot of a power-of-two table in its first 2^LOG2T
+// probes.
+//
 // Symbolic insert of a key into an open-addressing table of 2^LOG2T int
 // slots (empty = -1). Returns 1 when the key was new. The probe sequence is
 // bounded by the table size.
-template <int LOG2T>
+template <int LOG2T, bool QUAD = false>
 __device__ __forceinline__ int sym_insert(int *table, int key, int *err) {
   constexpr unsigned MASK = (1u << LOG2T) - 1u;
   unsigned h = hash_slot<LOG2T>(key);
@@ -96,7 +103,7 @@ __device__ __forceinline__ int sym_insert(int *table, int key, int *err) {
       if (old == kEmpty) return 1;
       if (old == key) return 0;
     }
-    h = (h + 1u) & MASK;
+    h = (h + (QUAD ? p : 0u) + 1u) & MASK;
   }
   atomicOr(err, ERR_PROBE);
   return 0;
@@ -107,7 +114,7 @@ __device__ __forceinline__ int sym_insert(int *table, int key, int *err) {
 // barrier, so the value update is a plain read-modify-write and the sum of
 // each entry is formed in the caller's step order (deterministic). Without
 // OWNED the value is added atomically.
-template <int LOG2T, bool OWNED>
+template <int LOG2T, bool OWNED, bool QUAD = false>
 __device__ __forceinline__ void num_insert(int *keys, double *vals, int key,
                                            double p, int *err) {
   constexpr unsigned MASK = (1u << LOG2T) - 1u;
@@ -128,14 +135,14 @@ __device__ __forceinline__ void num_insert(int *keys, double *vals, int key,
       }
       return;
     }
-    h = (h + 1u) & MASK;
+    h = (h + (QUAD ? q : 0u) + 1u) & MASK;
   }
   atomicOr(err, ERR_PROBE);
 }
 
 // Slot of `key` in (keys), inserting it when absent; -1 (and the error word)
 // when the probe sequence is exhausted.
-template <int LOG2T>
+template <int LOG2T, bool QUAD = false>
 __device__ __forceinline__ int num_slot(int *keys, int key, int *err) {
   constexpr unsigned MASK = (1u << LOG2T) - 1u;
   unsigned h = hash_slot<LOG2T>(key);
@@ -147,7 +154,7 @@ __device__ __forceinline__ int num_slot(int *keys, int key, int *err) {
       const int old = atomicCAS(keys + h, kEmpty, key);
       if (old == kEmpty || old == key) return (int)h;
     }
-    h = (h + 1u) & MASK;
+    h = (h + (QUAD ? q : 0u) + 1u) & MASK;
   }
   atomicOr(err, ERR_PROBE);
   return -1;

@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(kNumBlockThreads)
     int mn = 0x7fffffff, mx = -1;
     row_products<kNumBlockThreads>(acol, aval, brpt, bcol, bval, a0, a1, rq,
                                    [&](int key, double a, double b) {
-      num_insert<LOG2T, false>(keys, vals, key, __dmul_rn(a, b), err);
+      num_insert<LOG2T, false, true>(keys, vals, key, __dmul_rn(a, b), err);
       mn = min(mn, key);
       mx = max(mx, key);
     });

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kWideThreads)
       row_products<kWideThreads>(acol, (const double *)nullptr, brpt, bcol,
                                  (const double *)nullptr, a0, a1, rq,
                                  [&](int c, double, double) {
-                                   nz += sym_insert<kWideLog2T>(table, c, err);
+                                   nz += sym_insert<kWideLog2T, true>(table, c, err);
                                  });
       total = block_sum(nz);
     } else {
