@@ -13,6 +13,8 @@
 #include "common.cuh"
 #include "internal.h"
 
+#include <algorithm>
+
 namespace nspb {
 
 // ---- B row order --------------------------------------------------------------
@@ -44,6 +46,9 @@ __global__ void __launch_bounds__(256)
               int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
               int *__restrict__ sym_counts,
               unsigned long long *__restrict__ total_ip) {
+  // persistent grid: bin counts and the total accumulate in shared memory and
+  // reach global memory once per block (one block per few rows made every
+  // block add into the same dozen counters)
   __shared__ int hist[kSymBins];
   __shared__ unsigned long long s_total;
   if (threadIdx.x < kSymBins) hist[threadIdx.x] = 0;
@@ -51,23 +56,26 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   auto tile = cg::tiled_partition<GA>(cg::this_thread_block());
   const int lane = tile.thread_rank();
-  const int row = (int)(((int64_t)blockIdx.x * 256 + threadIdx.x) / GA);
-  long long ip = 0;
-  if (row < n) {
+  constexpr int kGroups = 256 / GA;
+  unsigned long long my_total = 0;
+  for (int row = blockIdx.x * kGroups + (int)threadIdx.x / GA; row < n;
+       row += gridDim.x * kGroups) {
     const int a0 = arpt[row], a1 = arpt[row + 1];
+    long long ip = 0;
     for (int j = a0 + lane; j < a1; j += GA) {
       const int k = ld_stream(acol + j);
       ip += brpt[k + 1] - brpt[k];
     }
+    ip = cg::reduce(tile, ip, cg::plus<long long>());
+    if (lane == 0) {
+      const int ub = (int)(ip < (long long)ncols_b ? ip : (long long)ncols_b);
+      row_nz[row] = ub;
+      if (row_ip) row_ip[row] = ip;
+      if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
+      my_total += (unsigned long long)ip;
+    }
   }
-  ip = cg::reduce(tile, ip, cg::plus<long long>());
-  if (lane == 0 && row < n) {
-    const int ub = (int)(ip < (long long)ncols_b ? ip : (long long)ncols_b);
-    row_nz[row] = ub;
-    if (row_ip) row_ip[row] = ip;
-    if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
-    if (ip) atomicAdd(&s_total, (unsigned long long)ip);
-  }
+  if (lane == 0 && my_total) atomicAdd(&s_total, my_total);
   __syncthreads();
   if (threadIdx.x < kSymBins && hist[threadIdx.x])
     atomicAdd(&sym_counts[threadIdx.x], hist[threadIdx.x]);
@@ -81,7 +89,8 @@ cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
   if (n <= 0) return cudaSuccess;
   const double avg = (double)A.nnz / (double)n;
   const int ga = avg > 24.0 ? 32 : avg > 12.0 ? 16 : avg > 6.0 ? 8 : 4;
-  const int grid = (int)(((int64_t)n * ga + 255) / 256);
+  const int grid = (int)std::min<int64_t>(((int64_t)n * ga + 255) / 256,
+                                          (int64_t)dev_info().sms * 8);
   switch (ga) {
     case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
     case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
