@@ -35,9 +35,11 @@ cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s);
 // row_nz[i] = min(intprod_i, ncols(B)); sym_counts[b] += rows of symbolic bin b
 // (rows with zero products are not binned); *total_ip += sum of intprod_i.
 // row_ip (optional) receives intprod_i as int64.
+// flags (may be NULL): when B is A, B_UNSORTED is set there as launch_check_sorted
+// would, from the rows read here.
 cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
                            int64_t *row_ip, int *sym_counts,
-                           unsigned long long *total_ip, cudaStream_t s);
+                           unsigned long long *total_ip, int *flags, cudaStream_t s);
 // Scatter rows into bin-contiguous order. kind 0: key = ub (symbolic bins),
 // kind 1: key = crpt[i+1]-crpt[i] (numeric bins). offsets: 16 bin starts.
 struct BinOffsets {

@@ -45,7 +45,9 @@ __global__ void __launch_bounds__(256)
               const int *__restrict__ brpt, int n, int ncols_b,
               int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
               int *__restrict__ sym_counts,
-              unsigned long long *__restrict__ total_ip) {
+              unsigned long long *__restrict__ total_ip, int *__restrict__ flags) {
+  // With flags (B is A): the order of every row read here is checked too,
+  // which is the B check of launch_check_sorted without a second read.
   // persistent grid: bin counts and the total accumulate in shared memory and
   // reach global memory once per block (one block per few rows made every
   // block add into the same dozen counters)
@@ -58,13 +60,25 @@ __global__ void __launch_bounds__(256)
   const int lane = tile.thread_rank();
   constexpr int kGroups = 256 / GA;
   unsigned long long my_total = 0;
+  int bad = 0;
   for (int row = blockIdx.x * kGroups + (int)threadIdx.x / GA; row < n;
        row += gridDim.x * kGroups) {
     const int a0 = arpt[row], a1 = arpt[row + 1];
     long long ip = 0;
-    for (int j = a0 + lane; j < a1; j += GA) {
-      const int k = ld_stream(acol + j);
-      ip += brpt[k + 1] - brpt[k];
+    int carry = -1;  // last column of the previous full round (columns are >= 0)
+    for (int jb = a0; jb < a1; jb += GA) {  // uniform across the group
+      const int j = jb + lane;
+      int k = -1;
+      if (j < a1) {
+        k = ld_stream(acol + j);
+        ip += brpt[k + 1] - brpt[k];
+      }
+      if (flags) {
+        int prev = tile.shfl_up(k, 1);
+        if (lane == 0) prev = carry;
+        if (j < a1 && k <= prev) bad = 1;
+        carry = tile.shfl(k, GA - 1);
+      }
     }
     ip = cg::reduce(tile, ip, cg::plus<long long>());
     if (lane == 0) {
@@ -76,7 +90,7 @@ __global__ void __launch_bounds__(256)
     }
   }
   if (lane == 0 && my_total) atomicAdd(&s_total, my_total);
-  __syncthreads();
+  if (__syncthreads_or(bad) && flags && threadIdx.x == 0) atomicOr(flags, B_UNSORTED);
   if (threadIdx.x < kSymBins && hist[threadIdx.x])
     atomicAdd(&sym_counts[threadIdx.x], hist[threadIdx.x]);
   if (threadIdx.x == 0 && s_total) atomicAdd(total_ip, s_total);
@@ -84,7 +98,7 @@ __global__ void __launch_bounds__(256)
 
 cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
                            int64_t *row_ip, int *sym_counts,
-                           unsigned long long *total_ip, cudaStream_t s) {
+                           unsigned long long *total_ip, int *flags, cudaStream_t s) {
   const int n = A.nrows;
   if (n <= 0) return cudaSuccess;
   const double avg = (double)A.nnz / (double)n;
@@ -92,10 +106,10 @@ cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
   const int grid = (int)std::min<int64_t>(((int64_t)n * ga + 255) / 256,
                                           (int64_t)dev_info().sms * 8);
   switch (ga) {
-    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
-    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
-    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
-    default: k_rowinfo<4><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip); break;
+    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
+    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
+    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
+    default: k_rowinfo<4><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
   }
   return cudaGetLastError();
 }

@@ -232,11 +232,14 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   int st = alloc_scratch();
   if (st) return st;
   mark(0);
-  if (!opts.assume_sorted) {
+  // B = A (the same arrays): the row walk of k_rowinfo checks B's order too
+  const bool same = A.rpt == B.rpt && A.col == B.col && A.nrows == B.nrows && A.nnz == B.nnz;
+  if (!opts.assume_sorted && !same) {
     if ((e = launch_check_sorted(B, &ctr->flags, s)) != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
-  if ((e = launch_rowinfo(A, B, row_nz, nullptr, ctr->sym_counts, &ctr->total_ip, s)) != cudaSuccess)
+  if ((e = launch_rowinfo(A, B, row_nz, nullptr, ctr->sym_counts, &ctr->total_ip,
+                          !opts.assume_sorted && same ? &ctr->flags : nullptr, s)) != cudaSuccess)
     return cuda_fail(e);
   ++launches;
   mark(1);
@@ -570,7 +573,7 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip, 
   }
   if ((st = call.alloc_scratch())) return st;
   cudaError_t e = launch_rowinfo(call.A, call.B, call.row_nz, d_row_ip, call.ctr->sym_counts,
-                                 &call.ctr->total_ip, call.s);
+                                 &call.ctr->total_ip, nullptr, call.s);
   if (e != cudaSuccess) return call.cuda_fail(e);
   if ((st = call.fetch_counters())) return st;
   if (total) *total = (int64_t)call.h.total_ip;

@@ -261,3 +261,26 @@ def test_stencil27_128_full_size_properties(cuda):
         assert_bitwise(C.val[a:b].cpu().numpy(), bval)
     del C
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("kind", ["sorted", "shuffled", "duplicate"])
+def test_same_operand_order_check(cuda, kind):
+    # A·A with one device matrix: the order of B (= A) is checked by the row
+    # walk that counts the intermediate products instead of a separate pass
+    P = nb.gen.powerlaw(6000, max_deg=300, seed=13)
+    col = P.col.copy()
+    rng = np.random.default_rng(5)
+    if kind == "shuffled":
+        for i in range(0, P.nrows, 7):
+            rng.shuffle(col[P.rowptr[i]:P.rowptr[i + 1]])
+    elif kind == "duplicate":
+        i = int(np.argmax(np.diff(P.rowptr)))
+        col[P.rowptr[i] + 1] = col[P.rowptr[i]]  # a repeated column breaks strict order
+    M = HostCSR(P.nrows, P.ncols, P.rowptr, col, P.val)
+    d = M.to_device()
+    C, st = nb.spgemm(d, d, return_stats=True)
+    assert st["b_sorted"] == (1 if kind == "sorted" else 0)
+    got = C.to_host()
+    rp, ocol, val = oracle.spgemm(M, M)
+    assert_same_structure(got.rowptr, got.col, rp, ocol)
+    assert_close(got.val, val, oracle.absbound(M, M, rp, ocol))
