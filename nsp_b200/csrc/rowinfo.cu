@@ -65,20 +65,12 @@ __global__ void __launch_bounds__(256)
        row += gridDim.x * kGroups) {
     const int a0 = arpt[row], a1 = arpt[row + 1];
     long long ip = 0;
-    int carry = -1;  // last column of the previous full round (columns are >= 0)
-    for (int jb = a0; jb < a1; jb += GA) {  // uniform across the group
-      const int j = jb + lane;
-      int k = -1;
-      if (j < a1) {
-        k = ld_stream(acol + j);
-        ip += brpt[k + 1] - brpt[k];
-      }
-      if (flags) {
-        int prev = tile.shfl_up(k, 1);
-        if (lane == 0) prev = carry;
-        if (j < a1 && k <= prev) bad = 1;
-        carry = tile.shfl(k, GA - 1);
-      }
+    for (int j = a0 + lane; j < a1; j += GA) {
+      const int k = ld_stream(acol + j);
+      ip += brpt[k + 1] - brpt[k];
+      // each entry against its predecessor, read directly: no dependence
+      // between rounds, so long rows keep their loads in flight
+      if (flags && j > a0 && k <= __ldg(acol + j - 1)) bad = 1;
     }
     ip = cg::reduce(tile, ip, cg::plus<long long>());
     if (lane == 0) {
