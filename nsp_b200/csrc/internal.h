@@ -36,10 +36,13 @@ cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s);
 // (rows with zero products are not binned); *total_ip += sum of intprod_i.
 // row_ip (optional) receives intprod_i as int64.
 // flags (may be NULL): when B is A, B_UNSORTED is set there as launch_check_sorted
-// would, from the rows read here.
+// would, from the rows read here. long_list / long_count (may be NULL; n ints and
+// a zeroed counter): rows of more than 1024 A entries are listed there and
+// counted by a second kernel, a block per row.
 cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
                            int64_t *row_ip, int *sym_counts,
-                           unsigned long long *total_ip, int *flags, cudaStream_t s);
+                           unsigned long long *total_ip, int *flags, int *long_list,
+                           int *long_count, cudaStream_t s);
 // Scatter rows into bin-contiguous order. kind 0: key = ub (symbolic bins),
 // kind 1: key = crpt[i+1]-crpt[i] (numeric bins). offsets: 16 bin starts.
 struct BinOffsets {

@@ -39,13 +39,18 @@ cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s) {
 }
 
 // ---- intermediate products and symbolic bins ---------------------------------
+// A rows longer than this are counted by a whole block (k_rowinfo_long), so
+// a power-law row of 10^4 entries does not leave one lane group walking it.
+constexpr int kRowinfoLong = 1024;
+
 template <int GA>
 __global__ void __launch_bounds__(256)
     k_rowinfo(const int *__restrict__ arpt, const int *__restrict__ acol,
               const int *__restrict__ brpt, int n, int ncols_b,
               int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
               int *__restrict__ sym_counts,
-              unsigned long long *__restrict__ total_ip, int *__restrict__ flags) {
+              unsigned long long *__restrict__ total_ip, int *__restrict__ flags,
+              int *__restrict__ long_list, int *__restrict__ long_count) {
   // With flags (B is A): the order of every row read here is checked too,
   // which is the B check of launch_check_sorted without a second read.
   // persistent grid: bin counts and the total accumulate in shared memory and
@@ -64,6 +69,10 @@ __global__ void __launch_bounds__(256)
   for (int row = blockIdx.x * kGroups + (int)threadIdx.x / GA; row < n;
        row += gridDim.x * kGroups) {
     const int a0 = arpt[row], a1 = arpt[row + 1];
+    if (long_list && a1 - a0 > kRowinfoLong) {  // left to k_rowinfo_long
+      if (lane == 0) long_list[atomicAdd(long_count, 1)] = row;
+      continue;
+    }
     long long ip = 0;
     for (int j = a0 + lane; j < a1; j += GA) {
       const int k = ld_stream(acol + j);
@@ -88,9 +97,56 @@ __global__ void __launch_bounds__(256)
   if (threadIdx.x == 0 && s_total) atomicAdd(total_ip, s_total);
 }
 
+// The rows k_rowinfo listed: one block per row, the same outputs.
+__global__ void __launch_bounds__(256)
+    k_rowinfo_long(const int *__restrict__ arpt, const int *__restrict__ acol,
+                   const int *__restrict__ brpt, int ncols_b, const int *__restrict__ long_list,
+                   const int *__restrict__ long_count, int *__restrict__ row_nz,
+                   int64_t *__restrict__ row_ip, int *__restrict__ sym_counts,
+                   unsigned long long *__restrict__ total_ip, int *__restrict__ flags) {
+  __shared__ int hist[kSymBins];
+  __shared__ long long red[8];
+  __shared__ unsigned long long s_total;
+  if (threadIdx.x < kSymBins) hist[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_total = 0ull;
+  __syncthreads();
+  const int count = *long_count;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int bad = 0;
+  for (int q = blockIdx.x; q < count; q += gridDim.x) {  // uniform across the block
+    const int row = long_list[q];
+    const int a0 = arpt[row], a1 = arpt[row + 1];
+    long long ip = 0;
+    for (int j = a0 + (int)threadIdx.x; j < a1; j += 256) {
+      const int k = ld_stream(acol + j);
+      ip += brpt[k + 1] - brpt[k];
+      if (flags && j > a0 && k <= __ldg(acol + j - 1)) bad = 1;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ip += __shfl_xor_sync(0xffffffffu, ip, o);
+    if (lane == 0) red[warp] = ip;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long t = 0;
+      for (int w = 0; w < 8; ++w) t += red[w];
+      const int ub = (int)(t < (long long)ncols_b ? t : (long long)ncols_b);
+      row_nz[row] = ub;
+      if (row_ip) row_ip[row] = t;
+      if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
+      s_total += (unsigned long long)t;
+    }
+    __syncthreads();
+  }
+  if (__syncthreads_or(bad) && flags && threadIdx.x == 0) atomicOr(flags, B_UNSORTED);
+  if (threadIdx.x < kSymBins && hist[threadIdx.x])
+    atomicAdd(&sym_counts[threadIdx.x], hist[threadIdx.x]);
+  if (threadIdx.x == 0 && s_total) atomicAdd(total_ip, s_total);
+}
+
 cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
                            int64_t *row_ip, int *sym_counts,
-                           unsigned long long *total_ip, int *flags, cudaStream_t s) {
+                           unsigned long long *total_ip, int *flags, int *long_list,
+                           int *long_count, cudaStream_t s) {
   const int n = A.nrows;
   if (n <= 0) return cudaSuccess;
   const double avg = (double)A.nnz / (double)n;
@@ -98,11 +154,16 @@ cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
   const int grid = (int)std::min<int64_t>(((int64_t)n * ga + 255) / 256,
                                           (int64_t)dev_info().sms * 8);
   switch (ga) {
-    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
-    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
-    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
-    default: k_rowinfo<4><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags); break;
+    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    default: k_rowinfo<4><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
   }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !long_list) return e;
+  k_rowinfo_long<<<dev_info().sms * 4, 256, 0, s>>>(A.rpt, A.col, B.rpt, B.ncols, long_list,
+                                                     long_count, row_nz, row_ip, sym_counts,
+                                                     total_ip, flags);
   return cudaGetLastError();
 }
 

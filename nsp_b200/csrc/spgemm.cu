@@ -238,8 +238,10 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     if ((e = launch_check_sorted(B, &ctr->flags, s)) != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
+  // perm is free until the bins are permuted: it holds the long-row list here
   if ((e = launch_rowinfo(A, B, row_nz, nullptr, ctr->sym_counts, &ctr->total_ip,
-                          !opts.assume_sorted && same ? &ctr->flags : nullptr, s)) != cudaSuccess)
+                          !opts.assume_sorted && same ? &ctr->flags : nullptr, perm,
+                          &ctr->long_rows, s)) != cudaSuccess)
     return cuda_fail(e);
   ++launches;
   mark(1);
@@ -573,7 +575,8 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip, 
   }
   if ((st = call.alloc_scratch())) return st;
   cudaError_t e = launch_rowinfo(call.A, call.B, call.row_nz, d_row_ip, call.ctr->sym_counts,
-                                 &call.ctr->total_ip, nullptr, call.s);
+                                 &call.ctr->total_ip, nullptr, call.perm, &call.ctr->long_rows,
+                                 call.s);
   if (e != cudaSuccess) return call.cuda_fail(e);
   if ((st = call.fetch_counters())) return st;
   if (total) *total = (int64_t)call.h.total_ip;

@@ -24,7 +24,8 @@ struct DevCounters {
   long long total_nnz;
   float max_row_err;
   int max_comp_deg;  // compensated mode: largest A-row degree of a pair row
-  int pad[2];
+  int long_rows;     // rows listed for the block-per-row intermediate-product count
+  int pad;
   int ticket[32];    // row tickets of the block-per-row launches (symbolic
                      // bin b at b, numeric bin b at 16 + b)
 };

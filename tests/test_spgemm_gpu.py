@@ -266,8 +266,11 @@ def test_stencil27_128_full_size_properties(cuda):
 @pytest.mark.parametrize("kind", ["sorted", "shuffled", "duplicate"])
 def test_same_operand_order_check(cuda, kind):
     # A·A with one device matrix: the order of B (= A) is checked by the row
-    # walk that counts the intermediate products instead of a separate pass
-    P = nb.gen.powerlaw(6000, max_deg=300, seed=13)
+    # walk that counts the intermediate products instead of a separate pass;
+    # rows of more than 1024 entries (counted by a block each) included, and
+    # the duplicate goes into the longest row
+    P = nb.gen.powerlaw(6000, max_deg=3000, seed=13)
+    assert np.diff(P.rowptr).max() > 1024
     col = P.col.copy()
     rng = np.random.default_rng(5)
     if kind == "shuffled":
