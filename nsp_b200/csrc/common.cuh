@@ -373,10 +373,6 @@ __device__ __forceinline__ int next_row(int *ticket, int count, int *s_slot) {
   return r < count ? r : count;
 }
 
-// Padded index of a bucket counter: one spare slot per 32 counters, so a
-// lane that owns a run of consecutive counters hits its own bank.
-__device__ __forceinline__ int cpad(int b) { return b + (b >> 5); }
-
 // Monotone bucket map of a key in [lo, lo+range) onto [0, nb): used to sort
 // the entries of one row (bucket scatter, then rank inside each bucket).
 __device__ __forceinline__ int bucket_of(int key, int lo, float scale, int nb) {
