@@ -468,6 +468,7 @@ int dev_alloc(T **p, size_t count) {
 // zeroed, operand entries concatenated, bin kernels, split.
 int group_numeric(PlanGroup &G, cudaStream_t s) {
   G.call.s = s;
+  if (G.call.n == 0) return NSPB_OK;  // no rows: no scratch, nothing to compute
   cudaError_t e = cudaMemsetAsync(G.call.ctr, 0, sizeof(DevCounters), s);
   if (e != cudaSuccess) return plan_fail(e);
   if (G.cat) {
@@ -536,7 +537,7 @@ int group_create(int count, const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr
   // the pass zeroes the device counters, so the symbolic counts are kept
   const DevCounters sym = G->call.h;
   if ((st = group_numeric(*G, s))) return st;
-  if ((st = G->call.fetch_counters())) return st;  // error word, redo counts
+  if (G->call.n > 0 && (st = G->call.fetch_counters())) return st;  // error word, redo counts
   DevCounters &hc = G->call.h;
   hc.total_nnz = sym.total_nnz;
   std::memcpy(hc.sym_counts, sym.sym_counts, sizeof(hc.sym_counts));
@@ -653,9 +654,12 @@ extern "C" int nspb_plan_execute(nspb_plan P, void *stream) {
   cudaError_t e = cudaGraphLaunch(P->exec, s);
   if (e != cudaSuccess) return plan_fail(e);
   if (!P->check) return NSPB_OK;
-  for (size_t g = 0; g < P->groups.size() && e == cudaSuccess; ++g)
-    e = cudaMemcpyAsync(P->h_err + g, &P->groups[g]->call.ctr->err, sizeof(int),
-                        cudaMemcpyDeviceToHost, s);
+  for (size_t g = 0; g < P->groups.size() && e == cudaSuccess; ++g) {
+    P->h_err[g] = 0;
+    if (P->groups[g]->call.ctr)  // groups without rows have no counters
+      e = cudaMemcpyAsync(P->h_err + g, &P->groups[g]->call.ctr->err, sizeof(int),
+                          cudaMemcpyDeviceToHost, s);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return plan_fail(e);
   for (size_t g = 0; g < P->groups.size(); ++g)

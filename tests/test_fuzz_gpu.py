@@ -39,7 +39,7 @@ shapes = st.tuples(st.integers(0, 300), st.integers(1, 400), st.integers(1, 500)
 
 def check(got, A, B):
     rp, col, val = oracle.spgemm(A, B)
-    h = got.to_host()
+    h = got if isinstance(got, HostCSR) else got.to_host()
     assert (h.nrows, h.ncols) == (A.nrows, B.ncols)
     assert_same_structure(h.rowptr, h.col, rp, col)
     assert_close(h.val, val, oracle.absbound(A, B, rp, col))
@@ -53,6 +53,8 @@ def test_random_products(cuda, s):
     A = random_csr(rng, n, k, da)
     B = random_csr(rng, k, m, db, unsorted, dup)
     check(nb.spgemm(A.to_device(), B.to_device()), A, B)
+    rp, col, val = nb.spgemm_host(A, B, nblocks=1 + seed % 5)  # host operands and result
+    check(HostCSR(A.nrows, B.ncols, rp, col, val), A, B)
 
 
 @settings(max_examples=10, deadline=None, suppress_health_check=list(HealthCheck))
