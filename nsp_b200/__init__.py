@@ -208,6 +208,8 @@ class Plan:
         self.stats = stats_dict(st)
 
         def view(ptr, cnt, ts, dt):
+            if cnt == 0:  # an empty product's pointer may sit one past an allocation
+                return torch.empty(0, dtype=dt, device="cuda")
             return torch.as_tensor(_PlanView(self, ptr, cnt, ts), device="cuda").view(dt)
         self.C = [DeviceCSR(c[p].nrows, c[p].ncols, view(c[p].rowptr, c[p].nrows + 1, "<i4", torch.int32),
                             view(c[p].col, c[p].nnz, "<i4", torch.int32),
