@@ -103,6 +103,14 @@ HostStage *host_stage() {
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Lanes per row group from the mean length of the B rows the products read.
+// Measured with the autotuner on B200: 32 lanes win from a mean of 8 entries up
+// (random, AMG and stencil products); 8 lanes only for B rows of about 4
+// entries when A has enough rows to fill the GPU with the smaller groups.
+static int pick_lanes(double mean_b_row, int a_rows) {
+  return (mean_b_row <= 6.0 && a_rows >= 65536) ? 8 : 32;
+}
+
 // ---- a call --------------------------------------------------------------------
 int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   nspb_default_opts(&opts);
@@ -144,8 +152,9 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   if (opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32) {
     lanes = opts.group_lanes;
   } else {
+    // until the intermediate products are counted (symbolic): B's mean row
     const double avg = B.nrows > 0 ? (double)B.nnz / (double)B.nrows : 0.0;
-    lanes = avg <= 8.0 ? 8 : avg <= 16.0 ? 16 : 32;
+    lanes = pick_lanes(avg, A.nrows);
   }
   return NSPB_OK;
 }
@@ -248,6 +257,10 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   if ((st = fetch_counters())) return st;
   b_sorted = opts.assume_sorted || !(h.flags & B_UNSORTED);
   intprod = (int64_t)h.total_ip;
+  // the mean length of the B rows actually read, weighted by how often A reads
+  // them: a block-diagonal batch mixes products whose B rows differ
+  if (!(opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32) && A.nnz > 0)
+    lanes = pick_lanes((double)intprod / (double)A.nnz, n);
   int nonempty = 0, binned = 0;
   BinOffsets off = offsets_of(h.sym_counts, kSymBins, &nonempty, &binned);
   const bool direct = nonempty == 1 && binned == n;
