@@ -50,6 +50,17 @@ struct BinOffsets {
 };
 cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets,
                         int *cursor, int *perm, cudaStream_t s);
+// Reorder row lists of perm (list i: perm[off[i] .. off[i]+count[i])) so that
+// rows of the heaviest weight class come first; weight as in launch_perm.
+// Lists of more than kOrderCap rows are left as they are.
+constexpr int kOrderCap = 32768;
+struct RowLists {
+  int off[16];
+  int count[16];
+  int n;
+};
+cudaError_t launch_order_rows(const int *key, int kind, const RowLists &lists, int *perm,
+                              cudaStream_t s);
 // Single-pass exclusive scan of row_nz into crpt[0..n] (crpt[n] = total) with
 // the numeric-bin histogram of the counts. Workspace: tile_state (zeroed,
 // scan_tiles(n) entries) and tile_ctr (zeroed).

@@ -202,6 +202,20 @@ int Call::cuda_fail(cudaError_t e) {
   return NSPB_ERR_CUDA;
 }
 
+cudaError_t Call::order_block_bins(const int *key, int kind, const int *counts, int first,
+                                   int end, const BinOffsets &off) {
+  RowLists lists{};
+  for (int b = first; b < end; ++b)
+    if (counts[b] > 1) {
+      lists.off[lists.n] = off.v[b];
+      lists.count[lists.n] = counts[b];
+      ++lists.n;
+    }
+  if (lists.n == 0) return cudaSuccess;
+  ++launches;
+  return launch_order_rows(key, kind, lists, perm, s);
+}
+
 int Call::fetch_counters() {
   HostStage *hs = stage ? stage : host_stage();
   if (!hs) return NSPB_ERR_ALLOC;
@@ -269,6 +283,8 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     if ((e = launch_perm(row_nz, n, 0, off, ctr->cursor_sym, perm, s)) != cudaSuccess)
       return cuda_fail(e);
     ++launches;
+    if ((e = order_block_bins(row_nz, 0, h.sym_counts, kSymGroupBins, kSymBins, off)) != cudaSuccess)
+      return cuda_fail(e);
   }
   for (int b = 0; b < kSymBins; ++b) {
     const int c = h.sym_counts[b];
@@ -304,6 +320,8 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     if ((e = launch_perm(crpt, n, 1, off, ctr->cursor_num, perm, s)) != cudaSuccess)
       return cuda_fail(e);
     ++launches;
+    if ((e = order_block_bins(crpt, 1, h.num_counts, kNumGroupBins, kNumBins, off)) != cudaSuccess)
+      return cuda_fail(e);
   }
   const bool comp = opts.precision == NSPB_PREC_FP32_COMP;
   const int nmax = comp ? comp_nmax(opts.comp_tol) : 0;

@@ -77,6 +77,9 @@ struct Call {
   int alloc_scratch();
   int cuda_fail(cudaError_t e);
   int fetch_counters();
+  // heaviest rows first in the block-per-row bins [first, end) of perm
+  cudaError_t order_block_bins(const int *key, int kind, const int *counts, int first, int end,
+                               const BinOffsets &off);
   int symbolic(int *crpt, int64_t *nnz_out);
   int prepare_numeric(const int *crpt);
   int numeric(const int *crpt, int *ccol, double *cval);

@@ -81,6 +81,37 @@ def test_every_bin(cuda):
     assert sum(1 for c in st["num_bins"] if c) >= 7
 
 
+def test_heaviest_rows_last(cuda):
+    # A-row degrees rising with the row index: every block-per-row list is
+    # reordered heaviest first before its launch (symbolic bins 8-11, numeric
+    # bins 6-9)
+    n, ncols = 1200, 3000
+    deg = np.linspace(0, 2600, n).astype(np.int64)
+    rng = np.random.default_rng(5)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(deg)
+    col = np.concatenate([np.sort(rng.choice(ncols, d, replace=False)) for d in deg]).astype(np.int32)
+    A = HostCSR(n, ncols, rp, col, rng.uniform(-1, 1, len(col)))
+    B = nb.gen.random(ncols, 60_000, 16, 16, seed=6)
+    got, st = check(A, B)
+    assert all(st["num_bins"][b] > 1 for b in (6, 7, 8, 9))
+    assert sum(st["sym_bins"][8:]) > 1
+
+
+def test_block_bin_longer_than_order_cap(cuda):
+    # 36,000 rows in numeric bin 6 (513..1024 entries), more than the 32,768
+    # rows a list may hold to be reordered, so that list stays in row order;
+    # 4,000 short rows make a second bin, so the rows are permuted at all
+    long_rows = nb.gen.random(36_000, 100_000, 40, 40, seed=31)
+    short_rows = nb.gen.random(4_000, 100_000, 4, 4, seed=33)
+    rp = np.concatenate([long_rows.rowptr, short_rows.rowptr[1:] + long_rows.nnz]).astype(np.int32)
+    A = HostCSR(40_000, 100_000, rp, np.concatenate([long_rows.col, short_rows.col]),
+                np.concatenate([long_rows.val, short_rows.val]))
+    B = nb.gen.random(100_000, 1_000_000, 16, 16, seed=32)
+    got, st = check(A, B)
+    assert st["num_bins"][6] > 32_768 and sum(st["num_bins"][:6]) > 0
+
+
 def test_rectangular_and_empty_rows(cuda):
     A = nb.gen.random(1000, 50, 0, 3, seed=4)   # many empty rows
     B = nb.gen.random(50, 10_000, 0, 2, seed=5)
