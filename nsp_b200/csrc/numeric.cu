@@ -243,6 +243,17 @@ __global__ void __launch_bounds__(256)
 // ---- block per row: warps over A entries, atomic accumulation ----------------------
 constexpr int kNumBlockThreads = 512;
 
+// Blocks per SM that the shared memory of a block-per-row kernel admits, given
+// to __launch_bounds__ as the minimum so that ptxas budgets registers for that
+// many blocks: without it ptxas kept these kernels at 32 registers a thread
+// (the budget of 2048 resident threads) and spilled, 290 bytes a thread in
+// k_num_rank, while their shared memory holds one or two blocks per SM.
+// k_num_block needs 20 bytes per table slot: 2^13 slots admit one block,
+// 2^12 two, smaller tables four (2048 threads).
+__host__ __device__ constexpr int num_block_minb(int log2t) {
+  return log2t >= 13 ? 1 : log2t == 12 ? 2 : 4;
+}
+
 // Exclusive scan of one int per thread over a 512-thread block; returns the
 // thread's exclusive prefix and the block total in *tot. red: 16 ints.
 __device__ __forceinline__ int block_exclusive_scan(int v, int *red, int *tot) {
@@ -272,7 +283,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *red, int *tot) {
 }
 
 template <int LOG2T, typename VT>
-__global__ void __launch_bounds__(kNumBlockThreads)
+__global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
     k_num_block(const int *__restrict__ arpt, const int *__restrict__ acol,
                 const VT *__restrict__ aval, const int *__restrict__ brpt,
                 const int *__restrict__ bcol, const VT *__restrict__ bval,
@@ -414,8 +425,13 @@ __host__ __device__ constexpr int rank_smem(int per_log2) {
   return (kRankThreads << per_log2) * 10 + kRankVals * 8;
 }
 
-template <typename VT>
-__global__ void __launch_bounds__(kRankThreads)
+// Blocks per SM the rank kernel's shared memory admits for the widest window:
+// windows of 2^19 columns or more (per_log2 >= 3, 131 KB and up) leave room for
+// one block, which may then use 64 registers a thread; narrower ones for two.
+__host__ __device__ constexpr int rank_minb(int per_log2) { return per_log2 >= 3 ? 1 : 2; }
+
+template <typename VT, int MINB>
+__global__ void __launch_bounds__(kRankThreads, MINB)
     k_num_rank(const int *__restrict__ arpt, const int *__restrict__ acol,
                const VT *__restrict__ aval, const int *__restrict__ brpt,
                const int *__restrict__ bcol, const VT *__restrict__ bval, int ncols,
@@ -547,12 +563,12 @@ static cudaError_t run_num_rank(const CsrDev &A, const CsrDev &B, const VT *av, 
                                 cudaStream_t s) {
   const int pl = rank_per_log2((int)std::min<long long>(B.ncols, kRankMaxCols));
   const int smem = rank_smem(pl);
-  const void *f = (const void *)k_num_rank<VT>;
-  const int grid = persistent_grid(f, kRankThreads, smem, count, 1);
+  auto kern = rank_minb(pl) == 1 ? k_num_rank<VT, 1> : k_num_rank<VT, 2>;
+  const int grid = persistent_grid((const void *)kern, kRankThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_rank<VT><<<grid, kRankThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, B.ncols,
-                                                  b_sorted ? 1 : 0, pl, crpt, ccol, cval, rows,
-                                                  count, err, redo, ticket);
+  kern<<<grid, kRankThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, B.ncols,
+                                        b_sorted ? 1 : 0, pl, crpt, ccol, cval, rows, count, err,
+                                        redo, ticket);
   return cudaGetLastError();
 }
 

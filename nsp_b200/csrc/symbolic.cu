@@ -84,7 +84,9 @@ constexpr int kLongWords = kLongBits / 32;
 constexpr int kWideLog2T = 15;      // hash table of 2^15 ints: the same 128 KB
 constexpr int kWideHashMax = 3 << (kWideLog2T - 2);
 
-__global__ void __launch_bounds__(kWideThreads)
+// 145 KB of shared memory a block: one block per SM, so the minimum of one
+// block lets ptxas use 64 registers a thread (it kept 32 without it)
+__global__ void __launch_bounds__(kWideThreads, 1)
     k_sym_wide(const int *__restrict__ arpt, const int *__restrict__ acol,
                const int *__restrict__ brpt, const int *__restrict__ bcol, int ncols,
                int b_sorted, const int *__restrict__ rows, int count,
