@@ -558,8 +558,8 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e2e_ms, "steps": args.e2e_steps,
                "entry": "nspb_spgemm_host (C ABI, pinned host operands and C; structure "
-                        "copied first, values during the symbolic phase, C copied back in "
-                        "row blocks under the numeric phase)"}
+                        "copied first, values in row chunks during the symbolic phase, C "
+                        "copied back in row blocks under the numeric phase)"}
 
     # ---- CPU baseline (rank 0 at N=1 only)
     cpu = None

@@ -61,6 +61,24 @@ def test_host_long_rows_and_unsorted(cuda):
     check(nb.spgemm_host(P, Pu, nblocks=4), P, Pu, exact=False)
 
 
+@pytest.mark.parametrize("nblocks", [2, 8, 40])
+def test_host_banded_value_chunks(cuda, nblocks):
+    # a banded A (rows reach only nearby B rows) with a separate B: row blocks
+    # wait for the value chunks of their own rows; empty row ranges in A give
+    # chunks without any column
+    A = nb.gen.stencil_slab(24, 24, 24, 0, 24, npts=7)
+    rp = A.rowptr.copy()
+    lo, hi = 3000, 7000  # rows [lo, hi) emptied
+    drop = rp[hi] - rp[lo]
+    keep = np.r_[0:rp[lo], rp[hi]:A.nnz]
+    rp[lo:hi + 1] = rp[lo]
+    rp[hi + 1:] -= drop
+    Ae = HostCSR(A.nrows, A.ncols, rp, A.col[keep], A.val[keep])
+    B = nb.gen.stencil(24, npts=27)
+    check(nb.spgemm_host(Ae, B, nblocks=nblocks), Ae, B, exact=True)
+    check(nb.spgemm_host(Pinned(B), Pinned(B), nblocks=nblocks), B, B, exact=True)
+
+
 def test_host_capacity(cuda):
     A = nb.gen.random(300, 200, 1, 8, seed=6)
     B = nb.gen.random(200, 100, 1, 8, seed=7)
