@@ -191,10 +191,11 @@ int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
 
 /* ---- host-memory operands --------------------------------------------------
  * C = A·B with A, B (nspb_csr_in whose pointers are HOST memory, row pointers
- * starting at 0) and C in host memory. Structure is copied first, values on
- * a second stream while the symbolic phase runs; the numeric phase runs in
- * `nblocks` row blocks (0 = 8) whose columns and values are copied back while
- * the next block is computed. Pinned host arrays give full-bandwidth,
+ * starting at 0) and C in host memory. Structure is copied first, values in
+ * row chunks on a second stream while the symbolic phase runs; the numeric
+ * phase runs in `nblocks` row blocks (0 = 16), each once the value chunks it
+ * reads are in, whose columns and values are copied back on a third stream
+ * while the next block is computed. Pinned host arrays give full-bandwidth,
  * overlapped copies. h_rowptr receives n+1 entries; h_col/h_val must hold
  * h_capacity entries: with fewer than nnz(C) (or NULL) only the row pointer
  * is written, *nnz_out tells the size and NSPB_ERR_CAPACITY is returned.
