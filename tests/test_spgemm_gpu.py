@@ -98,6 +98,24 @@ def test_heaviest_rows_last(cuda):
     assert sum(st["sym_bins"][8:]) > 1
 
 
+def test_long_rows_wide_column_space(cuda):
+    # B with more than 2^18 columns: the long-row kernel runs one block per SM
+    # (64 registers a thread) with a bitmap over all 500,000 columns; 927 rows
+    # of more than 6,144 entries add into C.val with fp64 atomics, and row 0
+    # (1.6 M products, 480 k entries) shares the launch with them
+    rng = np.random.default_rng(8)
+    n, k, m = 1500, 300_000, 500_000
+    deg = rng.integers(0, 2000, n)
+    deg[0] = 200_000
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(deg)
+    col = np.concatenate([np.sort(rng.choice(k, d, replace=False)) for d in deg]).astype(np.int32)
+    A = HostCSR(n, k, rp, col, rng.uniform(-1, 1, len(col)))
+    B = nb.gen.random(k, m, 4, 12, seed=9)
+    got, st = check(A, B)
+    assert st["num_bins"][9] > 100
+
+
 def test_block_bin_longer_than_order_cap(cuda):
     # 36,000 rows in numeric bin 6 (513..1024 entries), more than the 32,768
     # rows a list may hold to be reordered, so that list stays in row order;
