@@ -79,6 +79,17 @@ def test_host_banded_value_chunks(cuda, nblocks):
     check(nb.spgemm_host(Pinned(B), Pinned(B), nblocks=nblocks), B, B, exact=True)
 
 
+def test_host_compensated_fp32(cuda):
+    # fp32 host operands in the compensated mode: each row block's numeric step
+    # takes its bins from the host row pointer in this mode too
+    P = nb.gen.powerlaw(20_000, max_deg=2000, seed=12, fp32=True)  # fp32-representable
+    P32 = HostCSR(P.nrows, P.ncols, P.rowptr, P.col, P.val.astype(np.float32))
+    res = nb.spgemm_host(P32, P32, nblocks=6, precision="fp32c")
+    rp, col, val = oracle.spgemm(P, P)
+    assert_same_structure(np.asarray(res[0]), np.asarray(res[1]), rp, col)
+    assert_close(np.asarray(res[2]), val, oracle.absbound(P, P, rp, col), tol=1e-10)
+
+
 def test_host_capacity(cuda):
     A = nb.gen.random(300, 200, 1, 8, seed=6)
     B = nb.gen.random(200, 100, 1, 8, seed=7)
