@@ -228,9 +228,11 @@ __global__ void __launch_bounds__(256)
       vals[rank] = bvals[q];
     }
     tile.sync();
+    // C is written once and not read here again: streaming (evict-first)
+    // stores leave L2 to the B rows the next rows gather
     for (int q = lane; q < n; q += G) {
-      ccol[c0 + q] = keys[q];
-      cval[c0 + q] = vals[q];
+      __stcs(ccol + c0 + q, keys[q]);
+      __stcs(cval + c0 + q, vals[q]);
     }
     tile.sync();
   }
@@ -384,8 +386,8 @@ __global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
     }
     __syncthreads();
     for (int q = threadIdx.x; q < n; q += kNumBlockThreads) {
-      ccol[c0 + q] = keys[q];
-      cval[c0 + q] = vals[q];
+      __stcs(ccol + c0 + q, keys[q]);
+      __stcs(cval + c0 + q, vals[q]);
     }
     __syncthreads();
   }
@@ -538,7 +540,7 @@ __global__ void __launch_bounds__(kRankThreads, MINB)
           while (m) {
             const int b = __ffsll((long long)m) - 1;
             m &= m - 1ull;
-            ccol[pos++] = w0 + (w << 6) + b;
+            __stcs(ccol + pos++, w0 + (w << 6) + b);
           }
         }
       }
@@ -577,7 +579,7 @@ __global__ void __launch_bounds__(kRankThreads, MINB)
       }
       __syncthreads();
       if (in_smem && !bad)
-        for (int i = threadIdx.x; i < total; i += kRankThreads) cval[off + i] = vals[i];
+        for (int i = threadIdx.x; i < total; i += kRankThreads) __stcs(cval + off + i, vals[i]);
       for (int i = 0; i < per; ++i) bm64[t0 + i] = 0ull;
       off += total;
       __syncthreads();  // bitmap clear and value copy-out before the next window
