@@ -93,11 +93,14 @@ __global__ void __launch_bounds__(256)
   int my_max_deg = 0, my_redo = 0;  // compensated mode, flushed once per group
   for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
     const int row = rows ? rows[r] : r;
+    // 16-byte stores: two values or four keys each (both arrays start on a
+    // 16-byte boundary)
 #pragma unroll 4
-    for (int s = lane; s < C::T; s += G) {
-      keys[s] = kEmpty;
-      vals[s] = 0.0;
-    }
+    for (int s = lane; s < C::T / 2; s += G)
+      reinterpret_cast<double2 *>(vals)[s] = make_double2(0.0, 0.0);
+#pragma unroll 2
+    for (int s = lane; s < C::T / 4; s += G)
+      reinterpret_cast<int4 *>(keys)[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
     tile.sync();
     const int a0 = arpt[row], a1 = arpt[row + 1];
     // compensated mode: pair accumulation when the row's Dot2 bound allows it

@@ -44,8 +44,10 @@ __global__ void __launch_bounds__(256)
   int *table = smem_sym + g * C::T;
   for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
     const int row = rows ? rows[r] : r;
+    // four slots per 16-byte store (each table starts on a 16-byte boundary)
+    int4 *t4 = reinterpret_cast<int4 *>(table);
 #pragma unroll 4
-    for (int s = lane; s < C::T; s += G) table[s] = kEmpty;
+    for (int s = lane; s < C::T / 4; s += G) t4[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
     tile.sync();
     const int a0 = arpt[row], a1 = arpt[row + 1];
     int nz = 0;
