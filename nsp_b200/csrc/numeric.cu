@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(256)
     // table in slot order while counting buckets; (2) scan the counts;
     // (3) scatter into the table's free upper half [H, H+n); (4) rank inside
     // each bucket, writing the sorted row back to [0, n).
-    for (int b = lane; b < C::NB; b += G) cnt[b] = 0;
+    for (int b = lane; b < C::NB / 4; b += G) reinterpret_cast<int4 *>(cnt)[b] = make_int4(0, 0, 0, 0);
     tile.sync();
     const float scale = n > 0 ? (float)C::NB / (float)((long long)mx - mn + 1) : 0.f;
     int occ_total = 0;
@@ -311,11 +311,13 @@ __global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
   int rows_done = 0;
   for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
-    for (int s = threadIdx.x; s < T; s += kNumBlockThreads) {
-      keys[s] = kEmpty;
-      vals[s] = 0.0;
-    }
-    for (int b = threadIdx.x; b < NB; b += kNumBlockThreads) cnt[b] = 0;
+    // 16-byte stores (vals, keys and cnt start on 16-byte boundaries)
+    for (int s = threadIdx.x; s < T / 2; s += kNumBlockThreads)
+      reinterpret_cast<double2 *>(vals)[s] = make_double2(0.0, 0.0);
+    for (int s = threadIdx.x; s < T / 4; s += kNumBlockThreads)
+      reinterpret_cast<int4 *>(keys)[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
+    for (int b = threadIdx.x; b < NB / 4; b += kNumBlockThreads)
+      reinterpret_cast<int4 *>(cnt)[b] = make_int4(0, 0, 0, 0);
     if (threadIdx.x == 0) {
       s_mn = 0x7fffffff;
       s_mx = -1;
