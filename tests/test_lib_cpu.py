@@ -98,3 +98,42 @@ int main(void) {
                      ctypes.sizeof(_lib.Opts), ctypes.sizeof(_lib.Stats),
                      ctypes.sizeof(_lib.HostCsr), ctypes.sizeof(_lib.TuneEntry), 8]
     assert int(out[7]) == _lib.PREC_FP64
+
+
+def _host_in(M, val_type=_lib.F64):
+    d = _lib.CsrIn()
+    d.nrows, d.ncols, d.nnz = M.nrows, M.ncols, int(M.rowptr[M.nrows])
+    d.rowptr, d.col, d.val = M.rowptr.ctypes.data, M.col.ctypes.data, M.val.ctypes.data
+    d.val_type = val_type
+    return d
+
+
+def test_host_entry_checks_arguments_before_the_device():
+    """nspb_spgemm_host rejects malformed host operands with
+    NSPB_ERR_INVALID before any CUDA call, so the same statuses come back with
+    or without a GPU."""
+    import numpy as np
+    A = nb.gen.random(50, 40, 1, 5, seed=1)
+    B = nb.gen.random(40, 30, 1, 5, seed=2)
+    rp = np.empty(A.nrows + 1, np.int32)
+    nnz = ctypes.c_int64(0)
+
+    def call(a, b, nnz_out=ctypes.byref(nnz), rowptr=rp.ctypes.data):
+        return nb.lib.nspb_spgemm_host(ctypes.byref(a), ctypes.byref(b), rowptr, None, None, 0,
+                                       nnz_out, 0, None)
+
+    a, b = _host_in(A), _host_in(B)
+    assert call(a, _host_in(B, val_type=_lib.F32)) == _lib.ERR_INVALID  # value types differ
+    assert call(_host_in(B), b) == _lib.ERR_INVALID                      # ncols(A) != nrows(B)
+    assert call(a, b, nnz_out=None) == _lib.ERR_INVALID
+    assert call(a, b, rowptr=None) == _lib.ERR_INVALID
+    bad = _host_in(A)
+    bad.nnz = A.nnz - 1                                                   # rowptr[n] != nnz
+    assert call(bad, b) == _lib.ERR_INVALID
+    shifted = A.rowptr + 1                                                # rowptr[0] != 0
+    s = _host_in(A)
+    s.rowptr = shifted.ctypes.data
+    assert call(s, b) == _lib.ERR_INVALID
+    import torch
+    if not torch.cuda.is_available():
+        assert call(a, b) == _lib.ERR_NO_DEVICE
