@@ -111,7 +111,10 @@ typedef struct {
   int32_t num_table_shift; /* 0: numeric row-group tables of twice the bin's
                             entry limit (load <= 1/2); 1: four times (load
                             <= 1/4); chosen by nspb_autotune              */
-  int32_t _reserved;
+  int32_t row_kernel;    /* row-group kernels: 0 = default, 1 = hash tables
+                            with an in-table bucket sort, 2 = staged walk with
+                            tables of four times the bin's row limit, 3 = the
+                            same with tables of twice the limit              */
 } nspb_opts;
 
 /* Per-call figures (all optional; pass NULL).                               */

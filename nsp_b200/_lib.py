@@ -54,7 +54,7 @@ class Opts(C.Structure):
                 ("check_errors", C.c_int32), ("group_lanes", C.c_int32),
                 ("timing", C.c_int32), ("batch_max_products", C.c_int32),
                 ("comp_tol", C.c_double), ("stream", C.c_void_p),
-                ("num_table_shift", C.c_int32), ("_reserved", C.c_int32)]
+                ("num_table_shift", C.c_int32), ("row_kernel", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -127,7 +127,7 @@ int block_numeric(const nspb_csr_in *Ab, const nspb_csr_in *dB, nspb_csr_out *Cb
   call.b_sorted = ob->assume_sorted != 0;
   call.num_counts_ready = true;
   call.h.total_nnz = Cb->nnz;
-  if ((st = run_numeric_mode(call, Cb))) return st;
+  if ((st = call.numeric(Cb->rowptr, Cb->col, Cb->val))) return st;
   k_fold_err<<<1, 1, 0, call.s>>>(&call.ctr->err, err);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? NSPB_OK : fail(e);

@@ -30,6 +30,14 @@ struct CsrDev {
 // Flag bits written by launch_check_sorted.
 enum : int { B_UNSORTED = 1 };
 
+// Compensated-mode parameters of a numeric launch (fp32 inputs).
+struct CompArgs {
+  int nmax;        // rows with at most nmax A entries accumulate error-free in
+                   // fp32 pairs; longer rows accumulate in fp64
+  int *redo;       // counter of rows accumulated in fp64
+  int *max_deg;    // largest A-row degree among the pair-accumulated rows
+};
+
 // ---- rowinfo.cu -----------------------------------------------------------------
 cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s);
 // row_nz[i] = min(intprod_i, ncols(B)); sym_counts[b] += rows of symbolic bin b
@@ -101,5 +109,20 @@ cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorte
                                     int *ccol, double *cval, const int *rows, int count,
                                     int nmax, int *redo, int *max_deg, int *err,
                                     int *ticket, int tshift, cudaStream_t s);
+
+// ---- rowgroup.cu ----------------------------------------------------------------
+// Row-group bins (symbolic bins < kSymGroupBins, numeric bins < kNumGroupBins)
+// with lane groups of `lanes` lanes. Numeric: B rows strictly increasing;
+// tshift 0 gives tables of four times the bin's row limit, -1 twice.
+cudaError_t launch_symbolic_rg(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+                               const int *rows, int count, int *row_nz, int *err,
+                               cudaStream_t s);
+cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, const CsrDev &A, const CsrDev &B,
+                              const int *crpt, int *ccol, double *cval, const int *rows,
+                              int count, int *err, cudaStream_t s);
+cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, const CsrDev &A,
+                                   const CsrDev &B, const int *crpt, int *ccol, double *cval,
+                                   const int *rows, int count, int nmax, int *redo, int *max_deg,
+                                   int *err, cudaStream_t s);
 
 }  // namespace nspb

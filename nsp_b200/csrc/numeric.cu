@@ -62,14 +62,6 @@ struct NumGroupCfg {
   static constexpr int PER = NB >= G ? NB / G : 1;  // scan counters per lane
 };
 
-// Compensated-mode parameters of a numeric launch (fp32 inputs).
-struct CompArgs {
-  int nmax;        // rows with at most nmax A entries accumulate error-free in
-                   // fp32 pairs; longer rows accumulate in fp64
-  int *redo;       // counter of rows accumulated in fp64
-  int *max_deg;    // largest A-row degree among the pair-accumulated rows
-};
-
 // VT: value type of A and B (double, or float in the compensated mode).
 // COMP: fp32 inputs with the error-free pair accumulation for short rows.
 template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>

@@ -289,8 +289,11 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   for (int b = 0; b < kSymBins; ++b) {
     const int c = h.sym_counts[b];
     if (c <= 0) continue;
-    e = launch_symbolic_bin(b, lanes, b_sorted, A, B, direct ? nullptr : perm + off.v[b], c,
-                            row_nz, &ctr->err, &ctr->ticket[b], s);
+    const int *rows = direct ? nullptr : perm + off.v[b];
+    e = (b < kSymGroupBins && use_rg())
+            ? launch_symbolic_rg(b, lanes, A, B, rows, c, row_nz, &ctr->err, s)
+            : launch_symbolic_bin(b, lanes, b_sorted, A, B, rows, c, row_nz, &ctr->err,
+                                  &ctr->ticket[b], s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
@@ -331,6 +334,16 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     const int *rows = direct ? nullptr : perm + off.v[b];
     int *ticket = &ctr->ticket[16 + b];
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
+    if (b < kNumGroupBins && b_sorted && use_rg()) {
+      const int rg_shift = opts.row_kernel == 3 ? -1 : 0;
+      e = comp ? launch_numeric_comp_rg(b, lanes, rg_shift, A, B, crpt, ccol, cval, rows, c, nmax,
+                                        &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
+               : launch_numeric_rg(b, lanes, rg_shift, A, B, crpt, ccol, cval, rows, c,
+                                   &ctr->err, s);
+      if (e != cudaSuccess) return cuda_fail(e);
+      ++launches;
+      continue;
+    }
     e = comp ? launch_numeric_comp_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows,
                                        c, nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err,
                                        ticket, tshift, s)
@@ -525,7 +538,7 @@ int nspb_spgemm_numeric(const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out
     own = true;
     C->capacity = C->nnz;
   }
-  st = run_numeric_mode(call, C);
+  st = call.numeric(C->rowptr, C->col, C->val);
   if (!st) st = call.finish(stats);
   if (st && own) {
     cudaStreamSynchronize(call.s);
@@ -567,7 +580,7 @@ int nspb_spgemm(const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
       st = NSPB_ERR_CAPACITY;
     }
   }
-  if (!st) st = run_numeric_mode(call, C);
+  if (!st) st = call.numeric(C->rowptr, C->col, C->val);
   if (!st) st = call.finish(stats);
   if (st) {
     cudaStreamSynchronize(call.s);

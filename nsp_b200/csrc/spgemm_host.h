@@ -68,6 +68,8 @@ struct Call {
   // opts.timing: events around rowinfo, symbolic, scan, numeric
   cudaEvent_t ev[8] = {};
   bool timing = false;
+  // row-group bins through the rowgroup.cu kernels (opts.row_kernel 2 or 3)
+  bool use_rg() const { return opts.row_kernel == 2 || opts.row_kernel == 3; }
   void mark(int i) {
     if (timing && ev[i]) cudaEventRecord(ev[i], s);
   }
@@ -87,8 +89,6 @@ struct Call {
   ~Call();
 };
 
-// Numeric step in the call's precision mode (fp64 or fp32-compensated).
-int run_numeric_mode(Call &call, nspb_csr_out *C);
 // Compensated mode: longest A row accumulated in fp32 pairs for a tolerance,
 // and the relative error bound of a pair row with n A entries.
 int comp_nmax(double tol);
