@@ -37,6 +37,9 @@ sys.path.insert(0, ROOT)
 
 L = 128
 SEED = 20261203
+# the row-group kernels the default call runs (dominant launches of the stencil product)
+NUM_KERNEL = "k_num_group"
+SYM_KERNEL = "k_sym_group"
 METRIC = "SpGEMM GFLOP/s, C=A*A, 27-point stencil 128^3, fp64"
 WORKLOAD = "stencil27_128^3_AxA_fp64"
 
@@ -51,16 +54,20 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--grid", type=int, default=128,
                    help="stencil edge L (default 128; smaller grids for profiler captures)")
-    p.add_argument("--workload", default="stencil27",
-                   choices=["stencil27", "amg_batch", "fp32c", "powerlaw"],
-                   help="stencil27: the headline line; amg_batch: batched vs one call per "
-                        "product; fp32c: compensated fp32 vs fp64 on the 27-point stencil")
-    p.add_argument("--fp32c-matrix", default="stencil", choices=["stencil", "powerlaw"],
-                   help="fp32c workload: 27-point stencil 160^3 or the power-law 1M matrix")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the batched / fp32c / reference-kernel lines (profiler captures)")
+    p.add_argument("--form-steps", type=int, default=3,
+                   help="timed steps of each form (after one warm-up step)")
+    p.add_argument("--only-form", default=None, choices=["batched", "fp32c", "reference_gpu",
+                                                          "powerlaw"],
+                   help="run one form alone (prints its object as the JSON line)")
+    p.add_argument("--fp32c-grid", type=int, default=160)
     p.add_argument("--pl-rows", type=int, default=1_000_000,
                    help="power-law matrix order (default 1M; smaller for profiler captures)")
     p.add_argument("--batch-count", type=int, default=256)
     p.add_argument("--batch-nmax", type=int, default=100_000)
+    p.add_argument("--row-kernel", type=int, default=0,
+                   help="opts.row_kernel of the timed calls (0 = the library default)")
     return p.parse_args()
 
 
@@ -80,161 +87,199 @@ def _timed(fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def run_amg_batch(args):
-    """Batched products (one block-diagonal pipeline) against one nspb_spgemm
-    call per product, on the 6 Galerkin products of the SA-AMG hierarchy of
-    the 27-point stencil on 96^3 plus `batch-count` random products."""
-    import torch
+class _StepTimer:
+    """Device time of single calls: synchronize, event, call, event, synchronize.
+    Work released after a call (freeing its outputs) happens outside the
+    measured span, for every arm alike."""
+
+    def __init__(self):
+        import torch
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def __call__(self, fn, steps, warmup, after=None):
+        import torch
+        for _ in range(warmup):
+            fn()
+            if after:
+                after()
+        total = 0.0
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            self.e0.record()
+            fn()
+            self.e1.record()
+            torch.cuda.synchronize()
+            total += self.e0.elapsed_time(self.e1)
+            if after:
+                after()
+        return total / steps
+
+
+def form_batched(args, index):
+    """Batched products against one nspb_spgemm call per product, on equal
+    work: both arms run the symbolic and numeric phases and allocate C on
+    every step (outputs are released outside the timed spans). Workloads: the
+    6 Galerkin products of the SA-AMG hierarchy of the 27-point stencil on
+    96^3, and those plus `batch-count` random products. Plan replays (the
+    symbolic phase and C's allocation done once, the numeric phase replayed
+    from a CUDA graph) are reported beside them."""
     import nsp_b200 as nb
     from nsp_b200 import amg
     t0 = time.time()
     pairs = amg.amg_batch(L=96, levels=4, seed=SEED)
     n_amg = len(pairs)
     pairs += amg.random_batch(args.batch_count, 1000, args.batch_nmax, 4, 32, seed=SEED)
-    setup_s = time.time() - t0
     dA = [a.to_device() for a, _ in pairs]
     dB = [b.to_device() for _, b in pairs]
-    ip = sum(nb.intprod(a, b)[1] for a, b in zip(dA, dB))
-    ip_amg = sum(nb.intprod(a, b)[1] for a, b in zip(dA[:n_amg], dB[:n_amg]))
+    setup_s = time.time() - t0
+    ips = [nb.intprod(a, b)[1] for a, b in zip(dA, dB)]
     keep = []
-
-    def batched():
-        keep.clear()
-        keep.append(nb.spgemm_batched(dA, dB))
-
-    def single():
-        keep.clear()
-        keep.extend(nb.spgemm(a, b) for a, b in zip(dA, dB))
-
-    def batched_amg():
-        keep.clear()
-        keep.append(nb.spgemm_batched(dA[:n_amg], dB[:n_amg]))
-
-    def single_amg():
-        keep.clear()
-        keep.extend(nb.spgemm(a, b) for a, b in zip(dA[:n_amg], dB[:n_amg]))
-
-    w = max(args.warmup, 1)
-    ms_b = _timed(batched, args.steps, w)
-    ms_s = _timed(single, args.steps, w)
-    ms_ba = _timed(batched_amg, args.steps, w)
-    ms_sa = _timed(single_amg, args.steps, w)
-    keep.clear()
-    # plans: symbolic phase and C allocated once, the numeric phase replayed
-    # from a CUDA graph (values re-read every replay)
-    plan = nb.Plan(dA, dB, check_errors=False)
-    ms_p = _timed(plan.execute, args.steps, w)
-    del plan
-    plan_amg = nb.Plan(dA[:n_amg], dB[:n_amg], check_errors=False)
-    ms_pa = _timed(plan_amg.execute, args.steps, w)
-    del plan_amg
-    print(json.dumps({
-        "metric": "batched SpGEMM GFLOP/s (AMG 96^3 Galerkin products + random products)",
-        "value": 2 * ip / ms_b / 1e6, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": w, "ms_per_step": ms_b, "higher_is_better": True, "dtype": "f64",
-        "data": f"synthetic (seed {SEED})",
-        "config": {"workload": "amg96_galerkin_x6_plus_random", "products": len(pairs),
-                   "random_products": args.batch_count, "random_n": [1000, args.batch_nmax],
-                   "intprod": ip, "setup_s": setup_s},
-        "one_call_per_product": {"value": 2 * ip / ms_s / 1e6, "ms_per_step": ms_s},
-        "speedup_vs_one_call_per_product": ms_s / ms_b,
-        "plan_replay": {"value": 2 * ip / ms_p / 1e6, "ms_per_step": ms_p,
-                        "speedup_vs_one_call_per_product": ms_s / ms_p},
-        "amg_only": {"products": n_amg, "intprod": ip_amg,
-                     "batched_gflops": 2 * ip_amg / ms_ba / 1e6, "batched_ms": ms_ba,
-                     "one_call_gflops": 2 * ip_amg / ms_sa / 1e6, "one_call_ms": ms_sa,
-                     "plan_replay_gflops": 2 * ip_amg / ms_pa / 1e6, "plan_replay_ms": ms_pa}}),
-        flush=True)
+    timer = _StepTimer()
+    steps, warm = args.form_steps, 1
+    out = {"config": {"workload": "amg96_galerkin_x6 + random products",
+                      "products": len(pairs), "amg_products": n_amg,
+                      "random_products": args.batch_count, "random_n": [1000, args.batch_nmax],
+                      "random_degrees": [4, 32], "setup_s": round(setup_s, 1),
+                      "timing": "device time of each call, C allocated inside both arms, "
+                                "outputs freed outside the timed spans"}}
+    clocks = Clocks(index)
+    clocks.start()
+    for name, sl in (("amg", slice(0, n_amg)), ("amg_plus_random", slice(0, len(pairs)))):
+        a_s, b_s, ip = dA[sl], dB[sl], float(sum(ips[sl]))
+        ms_b = timer(lambda: keep.append(nb.spgemm_batched(a_s, b_s)), steps, warm, keep.clear)
+        ms_s = timer(lambda: keep.extend(nb.spgemm(a, b) for a, b in zip(a_s, b_s)), steps, warm,
+                     keep.clear)
+        plan = nb.Plan(a_s, b_s, check_errors=False)
+        ms_p = timer(plan.execute, steps, warm)
+        del plan
+        out[name] = {"intprod": int(ip),
+                     "batched": {"ms": ms_b, "gflops": 2 * ip / ms_b / 1e6},
+                     "one_call_per_product": {"ms": ms_s, "gflops": 2 * ip / ms_s / 1e6},
+                     "speedup_batched_vs_one_call": ms_s / ms_b,
+                     "plan_replay": {"ms": ms_p, "gflops": 2 * ip / ms_p / 1e6,
+                                     "speedup_vs_one_call": ms_s / ms_p}}
+    out["clocks"] = clocks.stop()
+    return out
 
 
-def run_powerlaw(args):
-    """C = A·A for the power-law matrix (n = 1M, Zipf alpha 2.1, mean degree
-    16, max 50k): every bin, including the long-row kernels."""
-    import torch
-    import nsp_b200 as nb
-    P = nb.gen.powerlaw(args.pl_rows, alpha=2.1, mean_deg=16.0, max_deg=50_000, seed=SEED)
-    dP = P.to_device()
-    C0, st0 = nb.spgemm(dP, dP, return_stats=True)
-    nnz = st0["nnz"]
-    del C0
-    out = nb.DeviceCSR(P.nrows, P.ncols, torch.empty(P.nrows + 1, dtype=torch.int32, device="cuda"),
-                       torch.empty(nnz, dtype=torch.int32, device="cuda"),
-                       torch.empty(nnz, dtype=torch.float64, device="cuda"))
-    phases = {}
-
-    def step():
-        _, s = nb.spgemm(dP, dP, out=out, check_errors=False, return_stats=True)
-
-    ms = _timed(step, args.steps, max(args.warmup, 1))
-    _, st = nb.spgemm(dP, dP, out=out, return_stats=True)
-    print(json.dumps({
-        "metric": f"SpGEMM GFLOP/s, C=A*A, power-law n={args.pl_rows} (alpha 2.1, mean 16, "
-                  "max 50k), fp64",
-        "value": 2 * st0["intprod"] / ms / 1e6, "unit": "GFLOP/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": ms,
-        "higher_is_better": True, "dtype": "f64", "data": f"synthetic (seed {SEED})",
-        "config": {"workload": f"powerlaw_{args.pl_rows}_AxA_fp64", "nnz_A": P.nnz,
-                   "xmin": nb.gen.powerlaw_xmin(), "intprod": st0["intprod"], "nnz_C": nnz,
-                   "sym_bins": st["sym_bins"], "num_bins": st["num_bins"]},
-        "effective_gbs": alg_bytes(P, P, nnz) / (ms * 1e-3) / 1e9}), flush=True)
+def _fp32c_errors(c32, c64, cabs):
+    """Error of the compensated result against the fp64 one: the largest
+    |c32 - c64| / sum_k |a_ik b_kj| over all entries, and the largest per-entry
+    relative error |c32 - c64| / |c64| over entries with |c64| above 1e-8 of
+    their sum_k |a b| (away from cancellation), with that entry count."""
+    d = (c32.val - c64.val).abs()
+    scaled = (d / cabs.val.clamp_min(1e-300)).max().item()
+    mask = c64.val.abs() > 1e-8 * cabs.val
+    rel = (d[mask] / c64.val.abs()[mask]).max().item() if bool(mask.any()) else 0.0
+    return {"max_err_scaled_by_sum_abs": scaled, "max_rel_err": rel,
+            "rel_err_entries": int(mask.sum().item()), "entries": int(c64.val.numel())}
 
 
-def run_fp32c(args):
-    """FP32 compensated against fp64 on the 27-point stencil (fp32-representable
-    values): time per product and the error of the fp32 path against the fp64
-    path, scaled by sum_k |a_ik b_kj| = (|A| |B|)_ij computed with the same
-    product on |A|."""
+def form_fp32c_one(args, index, which):
+    """FP32 compensated against fp64 on one matrix (fp32-representable values):
+    C preallocated for both paths, full products timed; errors per matrix."""
     import torch
     import nsp_b200 as nb
     from nsp_b200.csr import HostCSR
-    Lc = args.grid if args.grid != 128 else 160
-    if args.fp32c_matrix == "powerlaw":
+    if which == "powerlaw":
         A = nb.gen.powerlaw(args.pl_rows, alpha=2.1, mean_deg=16.0, max_deg=50_000, seed=SEED,
                             fp32=True)
-        label, wl = (f"power-law n={args.pl_rows} (alpha 2.1, mean 16, max 50k)",
-                     f"powerlaw_{args.pl_rows}_AxA")
+        wl = f"powerlaw_{args.pl_rows}_AxA"
     else:
-        A = nb.gen.stencil(Lc, npts=27, seed=SEED, fp32=True)
-        label, wl = f"27-point stencil {Lc}^3", f"stencil27_{Lc}^3_AxA"
-    data = f"synthetic ({label}, fp32-representable values, seed {SEED})"
+        A = nb.gen.stencil(args.fp32c_grid, npts=27, seed=SEED, fp32=True)
+        wl = f"stencil27_{args.fp32c_grid}^3_AxA"
     d64 = A.to_device()
     d32 = HostCSR(A.nrows, A.ncols, A.rowptr, A.col, A.val.astype(np.float32)).to_device()
     ip = nb.intprod(d64, d64)[1]
-    w = max(args.warmup, 1)
-    # C sized once and preallocated for both paths (fp64 values in both)
-    nnz = nb.spgemm_symbolic(d64, d64)[1]
+    rp, nnz = nb.spgemm_symbolic(d64, d64)
 
     def alloc():
-        return nb.DeviceCSR(A.nrows, A.ncols,
-                            torch.empty(A.nrows + 1, dtype=torch.int32, device="cuda"),
+        return nb.DeviceCSR(A.nrows, A.ncols, torch.empty_like(rp),
                             torch.empty(nnz, dtype=torch.int32, device="cuda"),
                             torch.empty(nnz, dtype=torch.float64, device="cuda"))
     o64, o32 = alloc(), alloc()
-    ms64 = _timed(lambda: nb.spgemm(d64, d64, out=o64, check_errors=False), args.steps, w)
     st = {}
 
     def f32():
         _, s_ = nb.spgemm(d32, d32, precision="fp32c", out=o32, check_errors=False,
                           return_stats=True)
         st.update(s_)
-
-    ms32 = _timed(f32, args.steps, w)
+    clocks = Clocks(index)
+    clocks.start()
+    ms64 = _timed(lambda: nb.spgemm(d64, d64, out=o64, check_errors=False), args.form_steps, 1)
+    ms32 = _timed(f32, args.form_steps, 1)
+    clk = clocks.stop()
+    nb.spgemm(d32, d32, precision="fp32c", out=o32)  # checked call
+    nb.spgemm(d64, d64, out=o64)
     dabs = nb.DeviceCSR(d64.nrows, d64.ncols, d64.rowptr, d64.col, d64.val.abs())
     cabs = nb.spgemm(dabs, dabs)
-    c64, c32 = o64, o32
-    assert torch.equal(c64.rowptr, c32.rowptr) and torch.equal(c64.col, c32.col)
-    err = ((c32.val - c64.val).abs() / cabs.val.clamp_min(1e-300)).max().item()
-    print(json.dumps({
-        "metric": f"SpGEMM GFLOP/s, C=A*A, {label}, fp32 compensated vs fp64",
-        "value": 2 * ip / ms32 / 1e6, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": w, "ms_per_step": ms32, "higher_is_better": True, "dtype": "f32 (compensated)",
-        "data": data,
-        "config": {"workload": wl, "intprod": ip, "nnz_C": c64.nnz},
-        "fp64": {"value": 2 * ip / ms64 / 1e6, "ms_per_step": ms64},
-        "speedup_vs_fp64": ms64 / ms32,
-        "max_err_vs_fp64_scaled_by_sum_abs": err,
-        "rows_in_fp64": st.get("rows_redone"), "a_priori_bound": st.get("max_row_err")}),
-        flush=True)
+    assert torch.equal(o64.rowptr, o32.rowptr) and torch.equal(o64.col, o32.col)
+    err = _fp32c_errors(o32, o64, cabs)
+    del o64, o32, cabs
+    return {"workload": wl, "intprod": ip, "nnz_C": nnz,
+            "fp32c": {"ms": ms32, "gflops": 2 * ip / ms32 / 1e6},
+            "fp64": {"ms": ms64, "gflops": 2 * ip / ms64 / 1e6},
+            "speedup_fp32c_vs_fp64": ms64 / ms32,
+            "errors_vs_fp64": err, "rows_in_fp64": st.get("rows_redone"),
+            "a_priori_bound": st.get("max_row_err"), "clocks": clk}
+
+
+def form_reference_gpu(args, index, A, dA):
+    """The reference's own nsp_spgemm_kernel_hash (built for sm_100a from the
+    reference sources into oracle/_ref by the oracle Makefile) against this
+    library's drop-in of the same entry point, on the same device inputs.
+    Both allocate C inside every call (the reference's contract, as timed by
+    its loc_time, src/spspmpi.cu:288-305). The reference's bins are checked
+    on the CPU first so it never reaches its unbounded chunk kernel
+    (nsp/src/nsp.cu:1725-1897)."""
+    import ctypes as C
+    import torch
+    import nsp_b200 as nb
+    import oracle
+    if not os.path.exists(oracle.REF_SO):
+        return {"unavailable": "oracle/_ref/libnsp_ref.so not built (reference sources absent)"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    ip, tot = oracle.intprod(A, A)
+    ok, why = make_golden.reference_bins_safe(A, A)
+    if not ok:
+        return {"unavailable": f"input reaches a reference path refused on the CPU: {why}"}
+    lib = C.CDLL(oracle.REF_SO)
+    lib.ref_nsp_time_device.restype = C.c_float
+    lib.ref_nsp_time_device.argtypes = [C.c_int] * 3 + [C.c_void_p] * 3 + [C.c_int] + \
+        [C.c_void_p] * 3 + [C.c_int] * 3 + [C.POINTER(C.c_int)]
+    nnz = C.c_int(0)
+    p = (dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr())
+    clocks = Clocks(index)
+    clocks.start()
+    ref_ms = lib.ref_nsp_time_device(A.nrows, A.ncols, A.ncols, *p, A.nnz, *p, A.nnz,
+                                     1, args.form_steps, C.byref(nnz))
+    torch.cuda.synchronize()
+    a = nb.sfcsr_of(dA)
+    cs = []
+
+    def ours():
+        c = nb.SfCSR()
+        nb.nsp_spgemm_kernel_hash(a, a, c)
+        cs.append(c)
+
+    def release():
+        for c in cs:
+            for ptr in (c.d_rpt, c.d_col, c.d_val):
+                nb.lib.nspb_free(C.c_void_p(ptr))
+        cs.clear()
+    ms = _StepTimer()(ours, args.form_steps, 1, release)
+    clk = clocks.stop()
+    flops = 2.0 * tot
+    return {"entry": "nsp_spgemm_kernel_hash(sfCSR*, sfCSR*, sfCSR*), C cudaMalloc'ed inside",
+            "workload": WORKLOAD, "nnz_C": nnz.value,
+            "reference_nsp": {"ms": ref_ms, "gflops": flops / ref_ms / 1e6,
+                              "build": "reference nsp.cu + nsp_calc_val_sort_rows.cu, "
+                                       "nvcc -O3 -arch sm_100a -DDOUBLE"},
+            "nspb_dropin": {"ms": ms, "gflops": flops / ms / 1e6},
+            "speedup_nspb_vs_reference": ref_ms / ms, "steps": args.form_steps,
+            "clocks": clk}
 
 
 def dist_env():
@@ -370,7 +415,11 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     import oracle
-    A, B = local_problem(0, 1)
+    from oracle import gen as ogen
+    # the same seeded stencil, built by the oracle's numpy restatement of the
+    # generator: this arm loads no part of the product library
+    A = ogen.stencil(L, 27, SEED)
+    B = A
     threads = os.cpu_count() or 1
     rows = sample_rows(A, B, threads, budget_s=max(2.0, 120.0 / max(args.steps + args.warmup, 1)))
     ip, _ = oracle.intprod(A, B, threads)
@@ -397,6 +446,59 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+def form_powerlaw(args, index):
+    """C = A·A for the power-law matrix (n = 1M, Zipf alpha 2.1, mean degree
+    16, max 50k), fp64, C preallocated: every bin, the long-row kernels too."""
+    import torch
+    import nsp_b200 as nb
+    P = nb.gen.powerlaw(args.pl_rows, alpha=2.1, mean_deg=16.0, max_deg=50_000, seed=SEED)
+    dP = P.to_device()
+    rp, nnz = nb.spgemm_symbolic(dP, dP)
+    out = nb.DeviceCSR(P.nrows, P.ncols, torch.empty_like(rp),
+                       torch.empty(nnz, dtype=torch.int32, device="cuda"),
+                       torch.empty(nnz, dtype=torch.float64, device="cuda"))
+    ip = nb.intprod(dP, dP)[1]
+    clocks = Clocks(index)
+    clocks.start()
+    ms = _timed(lambda: nb.spgemm(dP, dP, out=out, check_errors=False,
+                                  row_kernel=args.row_kernel), args.form_steps, 1)
+    clk = clocks.stop()
+    _, st = nb.spgemm(dP, dP, out=out, return_stats=True, row_kernel=args.row_kernel)
+    return {"workload": f"powerlaw_{args.pl_rows}_AxA_fp64", "nnz_A": P.nnz, "intprod": ip,
+            "nnz_C": nnz, "ms": ms, "gflops": 2 * ip / ms / 1e6,
+            "effective_gbs": alg_bytes(P, P, nnz) / (ms * 1e-3) / 1e9,
+            "sym_bins": st["sym_bins"], "num_bins": st["num_bins"], "clocks": clk}
+
+
+def _guarded(fn, *a):
+    """A form's object, or its error: a failing form does not take the
+    headline line with it (the error is in the line)."""
+    import torch
+    try:
+        r = fn(*a)
+    except Exception as ex:  # noqa: BLE001
+        r = {"error": f"{type(ex).__name__}: {ex}"}
+    torch.cuda.empty_cache()
+    return r
+
+
+def run_only_form(args, local):
+    import torch
+    torch.cuda.set_device(local)
+    if args.only_form == "batched":
+        res = form_batched(args, local)
+    elif args.only_form == "fp32c":
+        res = {"stencil": form_fp32c_one(args, local, "stencil"),
+               "powerlaw": form_fp32c_one(args, local, "powerlaw")}
+    elif args.only_form == "powerlaw":
+        res = form_powerlaw(args, local)
+    else:
+        import nsp_b200 as nb
+        A = nb.gen.stencil(L, npts=27, seed=SEED)
+        res = form_reference_gpu(args, local, A, A.to_device())
+    print(json.dumps({"form": args.only_form, **res}), flush=True)
+
+
 def main():
     global L, METRIC, WORKLOAD
     args = parse()
@@ -407,12 +509,8 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
-    if args.workload == "amg_batch":
-        return run_amg_batch(args)
-    if args.workload == "fp32c":
-        return run_fp32c(args)
-    if args.workload == "powerlaw":
-        return run_powerlaw(args)
+    if args.only_form:
+        return run_only_form(args, local)
 
     import ctypes as C
     import torch
@@ -468,6 +566,7 @@ def main():
     c_out.capacity = nnz_c
     opts = nb.make_opts(check_errors=False, stream=stream)
     opts.timing = 1
+    opts.row_kernel = args.row_kernel
     stats = _lib.Stats()
 
     def step():
@@ -512,11 +611,11 @@ def main():
     if dominant == "numeric":
         kbytes = alg_bytes(Ah, Bh, nnz_c)
         kms = phase["ms_numeric"]
-        kname = "k_num_group"
+        kname = NUM_KERNEL
     else:
         kbytes = 4 * (Ah.nrows + 1) + 4 * Ah.nnz + 4 * (Bh.nrows + 1) + 4 * Bh.nnz + 4 * Ah.nrows
         kms = phase["ms_symbolic"]
-        kname = "k_sym_group"
+        kname = SYM_KERNEL
     achieved = kbytes / (kms * 1e-3) / 1e9 if kms > 0 else 0.0
     traffic = profiled_traffic(kname)
 
@@ -598,6 +697,15 @@ def main():
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if world == 1 and not args.no_forms:
+            line["reference_gpu"] = _guarded(form_reference_gpu, args, local, Ah, dA)
+            del out, dA, dB
+            torch.cuda.empty_cache()
+            line["forms"] = {
+                "batched": _guarded(form_batched, args, local),
+                "fp32c": {"stencil": _guarded(form_fp32c_one, args, local, "stencil"),
+                          "powerlaw": _guarded(form_fp32c_one, args, local, "powerlaw")},
+                "powerlaw_fp64": _guarded(form_powerlaw, args, local)}
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

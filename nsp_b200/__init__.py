@@ -32,7 +32,7 @@ def _stream_ptr(stream):
 
 
 def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group_lanes=0,
-              comp_tol=1e-10, stream=None, table_shift=0) -> Opts:
+              comp_tol=1e-10, stream=None, table_shift=0, row_kernel=0) -> Opts:
     o = Opts()
     lib.nspb_default_opts(C.byref(o))
     o.precision = precision
@@ -42,6 +42,7 @@ def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group
     o.comp_tol = float(comp_tol)
     o.stream = _stream_ptr(stream)
     o.num_table_shift = int(table_shift)
+    o.row_kernel = int(row_kernel)
     return o
 
 
@@ -54,14 +55,15 @@ def stats_dict(s: Stats) -> dict:
 def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,
            stream=None, check_errors: bool = True, assume_sorted: bool = False,
            group_lanes: int = 0, comp_tol: float = 1e-10, return_stats: bool = False,
-           table_shift: int = 0):
+           table_shift: int = 0, row_kernel: int = 0):
     """C = A·B on the current CUDA device through nspb_spgemm.
 
     With `out` given, its tensors are used as C's arrays (capacity = their
     length); otherwise the library allocates C (freed with the tensors)."""
     import torch
     prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
-    o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream, table_shift)
+    o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream, table_shift,
+                  row_kernel)
     a, b = A.as_in(), B.as_in()
     c = CsrOut()
     if out is not None:
