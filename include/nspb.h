@@ -166,12 +166,16 @@ int nspb_spgemm_numeric(const nspb_csr_in *A, const nspb_csr_in *B,
  * memory reserved up front, a process near the HBM limit). C->rowptr, C->col
  * and C->val must be supplied, with C->capacity entries in col/val
  * (NSPB_ERR_CAPACITY with C->nnz = the size needed when too small). Scratch
- * comes from a fixed 32 MiB device array reserved when the library loads, so
- * A may have at most about 4.19 million rows (4,000,000 always fit); larger
- * inputs get NSPB_ERR_CAPACITY before any GPU work. Calls share that array:
- * calls whose GPU work overlaps race, so serialise them. The first call on
- * each device looks up the array's device address; make it before any stream
- * capture begins.                                                            */
+ * comes from a fixed 32 MiB device array inside the library, so A may have at
+ * most about 4.19 million rows (4,000,000 always fit); larger inputs get
+ * NSPB_ERR_CAPACITY with C->nnz = -1 before any GPU work. Calls share that
+ * array: calls whose GPU work overlaps race, so serialise them. The first
+ * call on each device looks up the array's device address, and CUDA's lazy
+ * module loading reserves the array's 32 MiB then (and loads the kernels at
+ * their first launch): make one small warm-up call at set-up, before any
+ * stream capture begins, so that later calls take no memory at all. The
+ * looked-up address assumes the device's primary context lives as long as
+ * the process (no cudaDeviceReset in between).                              */
 int nspb_spgemm_noalloc(const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
                         nspb_stats *stats);

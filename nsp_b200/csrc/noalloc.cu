@@ -7,14 +7,17 @@
 // a real-time loop whose device memory is reserved up front, or a process
 // running close to the HBM limit where a surprise allocation would fail.
 // They pass C's arrays in, and the call's scratch (row counts, the bin
-// permutation, counters and scan tile states) comes from one fixed array
-// that the library reserves in device memory when it is loaded.
+// permutation, counters and scan tile states) comes from one fixed array in
+// device memory inside the library (reserved at the first call on each
+// device, see below).
 //
 // The array is a file-scope __device__ variable of kNoAllocScratch bytes;
 // every GPU that loads this library holds it until the process exits. A call
 // needs 8 bytes per row of A plus a few KB (see Call::alloc_scratch), so A may
 // have at most about 4.19 million rows (4,000,000 is always accepted); larger
-// inputs are rejected with NSPB_ERR_CAPACITY before any GPU work starts.
+// inputs are rejected with NSPB_ERR_CAPACITY and C->nnz = -1 before any GPU
+// work starts (a C too small for nnz(C) gives NSPB_ERR_CAPACITY with C->nnz =
+// the entries needed, so the two cases are told apart).
 //
 // All calls on a device share the one array and it keeps the previous
 // call's contents: each call clears the counters and scan states it reads
@@ -27,6 +30,22 @@
 // that device current, looks the address up with cudaGetSymbolAddress and
 // keeps it; later calls reuse it. Make that first call before any stream
 // capture begins.
+//
+// When the memory is taken: CUDA loads a library's device code lazily by
+// default (CUDA_MODULE_LOADING=LAZY), module by module. The array lives in
+// this file's module, which is loaded by that first symbol lookup, so the
+// 32 MiB are reserved at the first call on a device, not when the library is
+// loaded; the product kernels' modules likewise load at their first launch.
+// A caller that must not see any allocation inside its working calls makes
+// one warm-up call at set-up time: a tiny product (a few rows) reserves the
+// array and loads every kernel the row-group path uses. (A zero-row call
+// reserves the array only.) With CUDA_MODULE_LOADING=EAGER everything loads
+// with the library.
+//
+// The cached address belongs to the device's primary context, which is
+// assumed to live as long as the process: after cudaDeviceReset (or a
+// released and recreated primary context) the cache is stale, so do not call
+// this entry point again in such a process.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -79,6 +98,10 @@ extern "C" int nspb_spgemm_noalloc(const nspb_csr_in *A, const nspb_csr_in *B,
   Call call;
   int st = call.init(A, B, &o);
   if (st) return st;
+  if (call.scratch_bytes() > kNoAllocScratch) {  // more rows than the array serves
+    C->nnz = -1;
+    return NSPB_ERR_CAPACITY;
+  }
   void *scratch = noalloc_scratch();
   if (!scratch) return NSPB_ERR_CUDA;
   call.ext_ws = static_cast<char *>(scratch);

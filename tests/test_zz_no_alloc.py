@@ -61,6 +61,8 @@ def test_noalloc_matches_spgemm_twice(cuda, name):
     dA, dB = A.to_device(), B.to_device()
     ref, rst = nb.spgemm(dA, dB, return_stats=True)
     ref = ref.to_host()
+    orp, ocol, _ = oracle.spgemm(A, B)
+    assert_same_structure(ref.rowptr, ref.col, orp, ocol)  # and both against the oracle
     deterministic = rst["b_sorted"] and sum(rst["num_bins"][6:]) == 0
     bound = oracle.absbound(A, B, ref.rowptr, ref.col)
     for _ in range(2):  # the second call sees the first call's scratch contents
@@ -72,6 +74,36 @@ def test_noalloc_matches_spgemm_twice(cuda, name):
             assert_bitwise(val[:nnz].cpu().numpy(), ref.val)
         else:
             assert_close(val[:nnz].cpu().numpy(), ref.val, bound)
+
+
+def test_noalloc_takes_no_device_memory(cuda):
+    """After a warm-up call (which reserves the fixed array and loads the
+    kernels), a call leaves the device's free memory unchanged, and its result
+    equals the oracle's."""
+    A = nb.gen.stencil(24, npts=27, seed=4)
+    dA = A.to_device()
+    rp, col, val = oracle.spgemm(A, A)
+    cap = len(col)
+    rowptr = torch.empty(A.nrows + 1, dtype=torch.int32, device="cuda")
+    ccol = torch.empty(cap, dtype=torch.int32, device="cuda")
+    cval = torch.empty(cap, dtype=torch.float64, device="cuda")
+    a = dA.as_in()
+    c = _lib.CsrOut()
+    c.rowptr, c.col, c.val = rowptr.data_ptr(), ccol.data_ptr(), cval.data_ptr()
+    c.capacity = cap
+    o = nb.make_opts(check_errors=True)
+
+    def call():
+        status = _fn(C.byref(a), C.byref(a), C.byref(c), C.byref(o), None)
+        torch.cuda.synchronize()
+        assert status == _lib.OK, nb.lib.nspb_strerror(status)
+    call()  # warm-up
+    free0 = torch.cuda.mem_get_info()[0]
+    call()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0
+    assert_same_structure(rowptr.cpu().numpy(), ccol.cpu().numpy(), rp, col)
+    assert_bitwise(cval.cpu().numpy(), val)
 
 
 def test_noalloc_capacity_reported(cuda):
@@ -86,8 +118,9 @@ def test_noalloc_rejects_more_rows_than_its_scratch(cuda):
     n = 4_300_000  # past the ~4.19 million rows the fixed scratch holds
     A = HostCSR(n, 8, np.zeros(n + 1, np.int32), np.zeros(0, np.int32), np.zeros(0))
     B = HostCSR(8, 8, np.zeros(9, np.int32), np.zeros(0, np.int32), np.zeros(0))
-    status, *_ = noalloc_product(A.to_device(), B.to_device(), 16)
+    status, nnz, *_ = noalloc_product(A.to_device(), B.to_device(), 16)
     assert status == _lib.ERR_CAPACITY
+    assert nnz == -1  # told apart from "C too small", which reports the size needed
     ok = HostCSR(4_000_000, 8, np.zeros(4_000_001, np.int32), np.zeros(0, np.int32),
                  np.zeros(0))
     status, nnz, rowptr, *_ = noalloc_product(ok.to_device(), B.to_device(), 16)
