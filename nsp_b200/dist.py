@@ -36,6 +36,27 @@ def row_offsets(n: int, world: int) -> list[int]:
     return [r * per for r in range(world)] + [n]
 
 
+def balanced_offsets(row_work, world: int) -> list[int]:
+    """Contiguous row blocks balanced by work: block r ends at the first row
+    where the prefix sum of `row_work` (the intermediate products of each row
+    of A, nspb_intprod) reaches (r+1)/world of the total. The reference splits
+    by row count (src/READ_MATRIX_MPI.cpp:256-270), which leaves the rank that
+    owns a power-law matrix's hub rows with most of the product. No block is
+    heavier than the ideal share plus the heaviest single row. Every rank
+    derives the same offsets from the same weights."""
+    import numpy as np
+    w = np.asarray(row_work, dtype=np.float64).ravel()
+    n = w.size
+    pre = np.concatenate(([0.0], np.cumsum(w)))
+    total = pre[-1]
+    if world <= 1 or n == 0 or total <= 0.0:
+        return row_offsets(n, max(world, 1))
+    targets = total * np.arange(1, world) / world
+    cuts = np.searchsorted(pre, targets, side="left")  # first prefix >= target
+    cuts = np.clip(cuts, 0, n)
+    return [0] + [int(c) for c in np.maximum.accumulate(cuts)] + [n]
+
+
 def _a2a(out, inp, out_splits, in_splits, group):
     import torch.distributed as dist
     dist.all_to_all_single(out, inp, out_splits, in_splits, group=group)

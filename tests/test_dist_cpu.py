@@ -33,7 +33,7 @@ def _problem(n, m, seed):
     return A, P
 
 
-def _rank_main(rank, world, port, n, m, seed, out_dir):
+def _rank_main(rank, world, port, n, m, seed, out_dir, balanced=False):
     import torch
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -41,9 +41,11 @@ def _rank_main(rank, world, port, n, m, seed, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     try:
         A, P = _problem(n, m, seed)
-        off = nd.row_offsets(n, world)
-        r0, r1 = off[rank], off[rank + 1]
-        Al, Pl = A.row_block(r0, r1), P.row_block(r0, r1)
+        off = nd.row_offsets(n, world)  # P keeps the reference's split
+        # A's rows: the same split, or blocks balanced by intermediate products
+        a_off = nd.balanced_offsets(oracle.intprod(A, P)[0], world) if balanced else off
+        r0, r1 = a_off[rank], a_off[rank + 1]
+        Al, Pl = A.row_block(r0, r1), P.row_block(off[rank], off[rank + 1])
         needed = np.unique(Al.col).astype(np.int32)
         rp, col, val = nd.exchange_rows(torch.from_numpy(Pl.rowptr), torch.from_numpy(Pl.col),
                                         torch.from_numpy(Pl.val), off, rank,
@@ -74,6 +76,31 @@ def test_halo_exchange_row_split(tmp_path, world):
     mp.start_processes(_rank_main, args=(world, _free_port(), 2500, 1800, 17, str(tmp_path)),
                        nprocs=world, start_method="spawn", join=True)
     assert sorted(os.listdir(tmp_path)) == [f"ok{r}" for r in range(world)]
+
+
+def test_halo_exchange_intprod_balanced_split(tmp_path):
+    """A split by the prefix of intermediate products while P keeps the
+    reference's split: rows of A and P then have different owners."""
+    import torch.multiprocessing as mp
+    world = 3
+    mp.start_processes(_rank_main, args=(world, _free_port(), 2500, 1800, 23, str(tmp_path), True),
+                       nprocs=world, start_method="spawn", join=True)
+    assert sorted(os.listdir(tmp_path)) == [f"ok{r}" for r in range(world)]
+
+
+def test_balanced_offsets_power_law():
+    P = nb.gen.powerlaw(20_000, max_deg=4000, seed=3)
+    ip, tot = oracle.intprod(P, P)
+    for world in (2, 3, 4, 8):
+        off = nd.balanced_offsets(ip, world)
+        assert off[0] == 0 and off[-1] == P.nrows and all(a <= b for a, b in zip(off, off[1:]))
+        work = [int(ip[a:b].sum()) for a, b in zip(off, off[1:])]
+        assert max(work) <= tot / world + ip.max()
+        # the reference's split by row count is less even on this matrix
+        even = nd.row_offsets(P.nrows, world)
+        assert max(work) <= max(int(ip[a:b].sum()) for a, b in zip(even, even[1:]))
+    assert nd.balanced_offsets([0, 0, 0], 2) == nd.row_offsets(3, 2)
+    assert nd.balanced_offsets([], 4) == [0, 0, 0, 0, 0]
 
 
 def test_row_offsets_match_reference_split():
