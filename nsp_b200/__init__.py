@@ -12,6 +12,7 @@ Entry points mirroring the reference (amavliut/nsp):
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 from . import gen, matio
 from ._lib import (F32, F64, PREC_FP32_COMP, PREC_FP64, CsrIn, CsrOut, NspbError, Opts,
@@ -32,7 +33,12 @@ def _stream_ptr(stream):
 
 
 def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group_lanes=0,
-              comp_tol=1e-10, stream=None, table_shift=0, row_kernel=0) -> Opts:
+              comp_tol=1e-10, stream=None, table_shift=0, row_kernel=None) -> Opts:
+    """nspb_opts for the Python entry points. row_kernel None takes
+    NSPB_ROW_KERNEL from the environment (0 when unset): the test suite runs
+    once per row-group kernel family that way."""
+    if row_kernel is None:
+        row_kernel = int(os.environ.get("NSPB_ROW_KERNEL", "0"), 0)
     o = Opts()
     lib.nspb_default_opts(C.byref(o))
     o.precision = precision
@@ -55,7 +61,7 @@ def stats_dict(s: Stats) -> dict:
 def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,
            stream=None, check_errors: bool = True, assume_sorted: bool = False,
            group_lanes: int = 0, comp_tol: float = 1e-10, return_stats: bool = False,
-           table_shift: int = 0, row_kernel: int = 0):
+           table_shift: int = 0, row_kernel: int | None = None):
     """C = A·B on the current CUDA device through nspb_spgemm.
 
     With `out` given, its tensors are used as C's arrays (capacity = their

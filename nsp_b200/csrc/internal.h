@@ -113,16 +113,29 @@ cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorte
 // ---- rowgroup.cu ----------------------------------------------------------------
 // Row-group bins (symbolic bins < kSymGroupBins, numeric bins < kNumGroupBins)
 // with lane groups of `lanes` lanes. Numeric: B rows strictly increasing;
-// tshift 0 gives tables of four times the bin's row limit, -1 twice.
-cudaError_t launch_symbolic_rg(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+// tshift 0 gives tables of four times the bin's row limit, -1 twice. depth:
+// B rows whose loads are issued together before their inserts (1, 2, 4, 8).
+cudaError_t launch_symbolic_rg(int bin, int lanes, int depth, const CsrDev &A, const CsrDev &B,
                                const int *rows, int count, int *row_nz, int *err,
                                cudaStream_t s);
-cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, const CsrDev &A, const CsrDev &B,
+cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
+                              const CsrDev &B,
                               const int *crpt, int *ccol, double *cval, const int *rows,
                               int count, int *err, cudaStream_t s);
-cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, const CsrDev &A,
+cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
                                    const CsrDev &B, const int *crpt, int *ccol, double *cval,
                                    const int *rows, int count, int nmax, int *redo, int *max_deg,
                                    int *err, cudaStream_t s);
+
+// ---- chunk.cu ---------------------------------------------------------------------
+// Row-group bins over column chunks (32 columns a chunk, a bit mask each).
+// Symbolic: *chunks receives the total number of chunks of the rows counted.
+// Numeric: fp64, B rows strictly increasing; depth as for the rowgroup kernels.
+cudaError_t launch_symbolic_chunk(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+                                  const int *rows, int count, int *row_nz,
+                                  unsigned long long *chunks, int *err, cudaStream_t s);
+cudaError_t launch_numeric_chunk(int bin, int lanes, int depth, const CsrDev &A,
+                                 const CsrDev &B, const int *crpt, int *ccol, double *cval,
+                                 const int *rows, int count, int *err, cudaStream_t s);
 
 }  // namespace nspb

@@ -82,7 +82,7 @@ struct SymRgCfg {
   static constexpr int SMEM = GPC * BYTES;
 };
 
-template <int G, int LOG2T>
+template <int G, int LOG2T, int D>
 __global__ void __launch_bounds__(256)
     k_sym_rg(const int *__restrict__ arpt, const int *__restrict__ acol,
              const int *__restrict__ brpt, const int *__restrict__ bcol,
@@ -117,21 +117,32 @@ __global__ void __launch_bounds__(256)
       tile.sync();
       const int na = min(G, a1 - ab);
       int t = 0;
-      // two B rows a round, both rows' keys loaded before either is inserted
-      for (; t + 2 <= na; t += 2) {
-        const int2 q0 = stage[t], q1 = stage[t + 1];
-        if (q0.y - q0.x <= G && q1.y - q1.x <= G) {
-          const int e0 = q0.x + lane, e1 = q1.x + lane;
-          const int k0 = e0 < q0.y ? __ldg(bcol + e0) : -1;
-          const int k1 = e1 < q1.y ? __ldg(bcol + e1) : -1;
-          if (k0 >= 0) nz += insert(k0);
-          if (k1 >= 0) nz += insert(k1);
+      // D B rows a round: every row's keys are loaded before any is inserted
+      for (; t + D <= na; t += D) {
+        int2 q[D];
+        bool shortrows = true;
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          q[i] = stage[t + i];
+          shortrows &= q[i].y - q[i].x <= G;
+        }
+        if (shortrows) {
+          int k[D];
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            const int e = q[i].x + lane;
+            k[i] = e < q[i].y ? __ldg(bcol + e) : -1;
+          }
+#pragma unroll
+          for (int i = 0; i < D; ++i)
+            if (k[i] >= 0) nz += insert(k[i]);
         } else {
-          for (int e = q0.x + lane; e < q0.y; e += G) nz += insert(__ldg(bcol + e));
-          for (int e = q1.x + lane; e < q1.y; e += G) nz += insert(__ldg(bcol + e));
+#pragma unroll 1
+          for (int i = 0; i < D; ++i)
+            for (int e = q[i].x + lane; e < q[i].y; e += G) nz += insert(__ldg(bcol + e));
         }
       }
-      if (t < na) {
+      for (; t < na; ++t) {
         const int2 q = stage[t];
         for (int e = q.x + lane; e < q.y; e += G) nz += insert(__ldg(bcol + e));
       }
@@ -145,40 +156,49 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-template <int G, int LOG2T>
+template <int G, int LOG2T, int D>
 static cudaError_t run_sym_rg(const CsrDev &A, const CsrDev &B, const int *rows, int count,
                               int *row_nz, int *err, cudaStream_t s) {
   using C = SymRgCfg<G, LOG2T>;
-  const void *f = (const void *)k_sym_rg<G, LOG2T>;
+  const void *f = (const void *)k_sym_rg<G, LOG2T, D>;
   const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_rg<G, LOG2T><<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, B.rpt, B.col, rows, count,
-                                                       row_nz, err);
+  k_sym_rg<G, LOG2T, D><<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, B.rpt, B.col, rows,
+                                                          count, row_nz, err);
   return cudaGetLastError();
 }
 
-template <int G>
+template <int G, int D>
 static cudaError_t sym_rg_bin(int bin, const CsrDev &A, const CsrDev &B, const int *rows,
                               int count, int *row_nz, int *err, cudaStream_t s) {
   switch (bin) {
-    case 0: return run_sym_rg<G, 5>(A, B, rows, count, row_nz, err, s);
-    case 1: return run_sym_rg<G, 6>(A, B, rows, count, row_nz, err, s);
-    case 2: return run_sym_rg<G, 7>(A, B, rows, count, row_nz, err, s);
-    case 3: return run_sym_rg<G, 8>(A, B, rows, count, row_nz, err, s);
-    case 4: return run_sym_rg<G, 9>(A, B, rows, count, row_nz, err, s);
-    case 5: return run_sym_rg<G, 10>(A, B, rows, count, row_nz, err, s);
-    case 6: return run_sym_rg<G, 11>(A, B, rows, count, row_nz, err, s);
-    default: return run_sym_rg<G, 12>(A, B, rows, count, row_nz, err, s);
+    case 0: return run_sym_rg<G, 5, D>(A, B, rows, count, row_nz, err, s);
+    case 1: return run_sym_rg<G, 6, D>(A, B, rows, count, row_nz, err, s);
+    case 2: return run_sym_rg<G, 7, D>(A, B, rows, count, row_nz, err, s);
+    case 3: return run_sym_rg<G, 8, D>(A, B, rows, count, row_nz, err, s);
+    case 4: return run_sym_rg<G, 9, D>(A, B, rows, count, row_nz, err, s);
+    case 5: return run_sym_rg<G, 10, D>(A, B, rows, count, row_nz, err, s);
+    case 6: return run_sym_rg<G, 11, D>(A, B, rows, count, row_nz, err, s);
+    default: return run_sym_rg<G, 12, D>(A, B, rows, count, row_nz, err, s);
   }
 }
 
-cudaError_t launch_symbolic_rg(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+template <int D>
+static cudaError_t sym_rg_lanes(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+                                const int *rows, int count, int *row_nz, int *err,
+                                cudaStream_t s) {
+  if (lanes == 8) return sym_rg_bin<8, D>(bin, A, B, rows, count, row_nz, err, s);
+  if (lanes == 16) return sym_rg_bin<16, D>(bin, A, B, rows, count, row_nz, err, s);
+  return sym_rg_bin<32, D>(bin, A, B, rows, count, row_nz, err, s);
+}
+
+cudaError_t launch_symbolic_rg(int bin, int lanes, int depth, const CsrDev &A, const CsrDev &B,
                                const int *rows, int count, int *row_nz, int *err,
                                cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  if (lanes == 8) return sym_rg_bin<8>(bin, A, B, rows, count, row_nz, err, s);
-  if (lanes == 16) return sym_rg_bin<16>(bin, A, B, rows, count, row_nz, err, s);
-  return sym_rg_bin<32>(bin, A, B, rows, count, row_nz, err, s);
+  if (depth >= 8) return sym_rg_lanes<8>(bin, lanes, A, B, rows, count, row_nz, err, s);
+  if (depth >= 4) return sym_rg_lanes<4>(bin, lanes, A, B, rows, count, row_nz, err, s);
+  return sym_rg_lanes<2>(bin, lanes, A, B, rows, count, row_nz, err, s);
 }
 
 // ---- numeric ---------------------------------------------------------------------
@@ -199,7 +219,7 @@ struct NumRgCfg {
   static constexpr int SMEM = GPC * BYTES;
 };
 
-template <int G, int LOG2H, int LOG2T, typename VT, bool COMP>
+template <int G, int LOG2H, int LOG2T, typename VT, bool COMP, int D>
 __global__ void __launch_bounds__(256)
     k_num_rg(const int *__restrict__ arpt, const int *__restrict__ acol,
              const VT *__restrict__ aval, const int *__restrict__ brpt,
@@ -252,31 +272,57 @@ __global__ void __launch_bounds__(256)
       }
       tile.sync();
       const int na = min(G, a1 - ab);
-      for (int t = 0; t < na; ++t) {
-        const int4 q = stage[t];
-        const double a = __hiloint2double(q.w, q.z);
-        for (int e = q.x + lane; e < q.y; e += G) {
-          const int key = __ldg(bcol + e);
-          const VT b = __ldg(bval + e);
-          bool fresh;
-          const int h = rg_slot<LOG2T>(keys, key, fresh, err);
-          if (h >= 0) {
-            if (pair) {
-              const float af = (float)a, bf = (float)b;
-              if (fresh) {
-                const float ph = __fmul_rn(af, bf);
-                vals2[h] = make_float2(ph, __fmaf_rn(af, bf, -ph));
-              } else {
-                float2 sc = vals2[h];
-                comp_add(sc, af, bf);
-                vals2[h] = sc;
-              }
-            } else {
-              const double p = __dmul_rn(a, (double)b);
-              vals[h] = __dadd_rn(fresh ? 0.0 : vals[h], p);
-            }
+      auto add = [&](int key, double a, VT b) {
+        bool fresh;
+        const int h = rg_slot<LOG2T>(keys, key, fresh, err);
+        if (h < 0) return;
+        if (pair) {
+          const float af = (float)a, bf = (float)b;
+          if (fresh) {
+            const float ph = __fmul_rn(af, bf);
+            vals2[h] = make_float2(ph, __fmaf_rn(af, bf, -ph));
+          } else {
+            float2 sc = vals2[h];
+            comp_add(sc, af, bf);
+            vals2[h] = sc;
+          }
+        } else {
+          const double p = __dmul_rn(a, (double)b);
+          vals[h] = __dadd_rn(fresh ? 0.0 : vals[h], p);
+        }
+      };
+      int t = 0;
+      if constexpr (D > 1) {
+        // D B rows a round: all their keys and values are loaded before the
+        // first insert; the inserts still go step by step in A-row order
+        for (; t + D <= na; t += D) {
+          int4 q[D];
+          bool shortrows = true;
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            q[i] = stage[t + i];
+            shortrows &= q[i].y - q[i].x <= G;
+          }
+          if (!shortrows) break;  // the step loop below takes the rest
+          int k[D];
+          VT b[D];
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            const int e = q[i].x + lane;
+            k[i] = e < q[i].y ? __ldg(bcol + e) : -1;
+            b[i] = e < q[i].y ? __ldg(bval + e) : VT(0);
+          }
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            if (k[i] >= 0) add(k[i], __hiloint2double(q[i].w, q[i].z), b[i]);
+            tile.sync();  // the next step may hit the same slots
           }
         }
+      }
+      for (; t < na; ++t) {
+        const int4 q = stage[t];
+        const double a = __hiloint2double(q.w, q.z);
+        for (int e = q.x + lane; e < q.y; e += G) add(__ldg(bcol + e), a, __ldg(bval + e));
         tile.sync();  // the next step may hit the same slots
       }
     }
@@ -392,25 +438,28 @@ __global__ void __launch_bounds__(256)
 template <int G, int LOG2H, int LOG2T, typename VT, bool COMP>
 static cudaError_t run_num_rg(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
                               const int *crpt, int *ccol, double *cval, const int *rows,
-                              int count, int *err, CompArgs comp, cudaStream_t s) {
+                              int count, int *err, CompArgs comp, int depth, cudaStream_t s) {
   using C = NumRgCfg<G, LOG2H, LOG2T>;
-  const void *f = (const void *)k_num_rg<G, LOG2H, LOG2T, VT, COMP>;
-  const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
+  auto kern = depth >= 4 ? k_num_rg<G, LOG2H, LOG2T, VT, COMP, 4>
+            : depth >= 2 ? k_num_rg<G, LOG2H, LOG2T, VT, COMP, 2>
+                         : k_num_rg<G, LOG2H, LOG2T, VT, COMP, 1>;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_rg<G, LOG2H, LOG2T, VT, COMP><<<grid, C::THREADS, C::SMEM, s>>>(
-      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, comp);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval,
+                                         rows, count, err, comp);
   return cudaGetLastError();
 }
 
 // Numeric bin b holds rows of at most 16 << b entries (H); the table has
 // 4H slots (load <= 1/4) or, with tshift = -1, 2H.
 template <int G, typename VT, bool COMP>
-static cudaError_t num_rg_bin(int bin, int tshift, const CsrDev &A, const CsrDev &B,
+static cudaError_t num_rg_bin(int bin, int tshift, int depth, const CsrDev &A, const CsrDev &B,
                               const VT *av, const VT *bv, const int *crpt, int *ccol,
                               double *cval, const int *rows, int count, int *err,
                               CompArgs comp, cudaStream_t s) {
 #define NSPB_NRG(L2H, L2T) \
-  run_num_rg<G, L2H, L2T, VT, COMP>(A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
+  run_num_rg<G, L2H, L2T, VT, COMP>(A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, \
+                                    depth, s)
   const bool big = tshift >= 0;
   switch (bin) {
     case 0: return big ? NSPB_NRG(4, 6) : NSPB_NRG(4, 5);
@@ -423,34 +472,35 @@ static cudaError_t num_rg_bin(int bin, int tshift, const CsrDev &A, const CsrDev
 #undef NSPB_NRG
 }
 
-cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, const CsrDev &A, const CsrDev &B,
+cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
+                              const CsrDev &B,
                               const int *crpt, int *ccol, double *cval, const int *rows,
                               int count, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   const CompArgs none{0, nullptr, nullptr};
   if (lanes == 8)
-    return num_rg_bin<8, double, false>(bin, tshift, A, B, A.val, B.val, crpt, ccol, cval, rows,
+    return num_rg_bin<8, double, false>(bin, tshift, depth, A, B, A.val, B.val, crpt, ccol, cval, rows,
                                         count, err, none, s);
   if (lanes == 16)
-    return num_rg_bin<16, double, false>(bin, tshift, A, B, A.val, B.val, crpt, ccol, cval, rows,
+    return num_rg_bin<16, double, false>(bin, tshift, depth, A, B, A.val, B.val, crpt, ccol, cval, rows,
                                          count, err, none, s);
-  return num_rg_bin<32, double, false>(bin, tshift, A, B, A.val, B.val, crpt, ccol, cval, rows,
+  return num_rg_bin<32, double, false>(bin, tshift, depth, A, B, A.val, B.val, crpt, ccol, cval, rows,
                                        count, err, none, s);
 }
 
-cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, const CsrDev &A,
+cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
                                    const CsrDev &B, const int *crpt, int *ccol, double *cval,
                                    const int *rows, int count, int nmax, int *redo, int *max_deg,
                                    int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   const CompArgs comp{nmax, redo, max_deg};
   if (lanes == 8)
-    return num_rg_bin<8, float, true>(bin, tshift, A, B, A.val32, B.val32, crpt, ccol, cval, rows,
+    return num_rg_bin<8, float, true>(bin, tshift, depth, A, B, A.val32, B.val32, crpt, ccol, cval, rows,
                                       count, err, comp, s);
   if (lanes == 16)
-    return num_rg_bin<16, float, true>(bin, tshift, A, B, A.val32, B.val32, crpt, ccol, cval,
+    return num_rg_bin<16, float, true>(bin, tshift, depth, A, B, A.val32, B.val32, crpt, ccol, cval,
                                        rows, count, err, comp, s);
-  return num_rg_bin<32, float, true>(bin, tshift, A, B, A.val32, B.val32, crpt, ccol, cval, rows,
+  return num_rg_bin<32, float, true>(bin, tshift, depth, A, B, A.val32, B.val32, crpt, ccol, cval, rows,
                                      count, err, comp, s);
 }
 

@@ -290,8 +290,11 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     const int c = h.sym_counts[b];
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
-    e = (b < kSymGroupBins && use_rg())
-            ? launch_symbolic_rg(b, lanes, A, B, rows, c, row_nz, &ctr->err, s)
+    e = (b < kSymGroupBins && use_chunk())
+            ? launch_symbolic_chunk(b, lanes, A, B, rows, c, row_nz, &ctr->total_chunks,
+                                    &ctr->err, s)
+        : (b < kSymGroupBins && use_rg())
+            ? launch_symbolic_rg(b, lanes, rg_depth(), A, B, rows, c, row_nz, &ctr->err, s)
             : launch_symbolic_bin(b, lanes, b_sorted, A, B, rows, c, row_nz, &ctr->err,
                                   &ctr->ticket[b], s);
     if (e != cudaSuccess) return cuda_fail(e);
@@ -334,11 +337,18 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     const int *rows = direct ? nullptr : perm + off.v[b];
     int *ticket = &ctr->ticket[16 + b];
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
-    if (b < kNumGroupBins && b_sorted && use_rg()) {
-      const int rg_shift = opts.row_kernel == 3 ? -1 : 0;
-      e = comp ? launch_numeric_comp_rg(b, lanes, rg_shift, A, B, crpt, ccol, cval, rows, c, nmax,
+    if (b < kNumGroupBins && b_sorted && !comp && use_chunk()) {
+      e = launch_numeric_chunk(b, lanes, rg_depth(), A, B, crpt, ccol, cval, rows, c, &ctr->err,
+                               s);
+      if (e != cudaSuccess) return cuda_fail(e);
+      ++launches;
+      continue;
+    }
+    if (b < kNumGroupBins && b_sorted && (use_rg() || (comp && use_chunk()))) {
+      const int rg_shift = (opts.row_kernel & 0xff) == 3 ? -1 : 0;
+      e = comp ? launch_numeric_comp_rg(b, lanes, rg_shift, rg_depth(), A, B, crpt, ccol, cval, rows, c, nmax,
                                         &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
-               : launch_numeric_rg(b, lanes, rg_shift, A, B, crpt, ccol, cval, rows, c,
+               : launch_numeric_rg(b, lanes, rg_shift, rg_depth(), A, B, crpt, ccol, cval, rows, c,
                                    &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;

@@ -26,6 +26,7 @@ struct DevCounters {
   int max_comp_deg;  // compensated mode: largest A-row degree of a pair row
   int long_rows;     // rows listed for the block-per-row intermediate-product count
   int pad;
+  unsigned long long total_chunks;  // column chunks of the rows the chunk kernels counted
   int ticket[32];    // row tickets of the block-per-row launches (symbolic
                      // bin b at b, numeric bin b at 16 + b)
 };
@@ -69,7 +70,10 @@ struct Call {
   cudaEvent_t ev[8] = {};
   bool timing = false;
   // row-group bins through the rowgroup.cu kernels (opts.row_kernel 2 or 3)
-  bool use_rg() const { return opts.row_kernel == 2 || opts.row_kernel == 3; }
+  bool use_rg() const { return (opts.row_kernel & 0xff) == 2 || (opts.row_kernel & 0xff) == 3; }
+  bool use_chunk() const { return (opts.row_kernel & 0xff) == 4; }
+  // loads issued ahead in the row-group walks: bits 8.. of row_kernel (0 = 2)
+  int rg_depth() const { return (opts.row_kernel >> 8) ? (opts.row_kernel >> 8) : 2; }
   void mark(int i) {
     if (timing && ev[i]) cudaEventRecord(ev[i], s);
   }
