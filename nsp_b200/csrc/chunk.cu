@@ -76,14 +76,53 @@ __device__ __forceinline__ int chunk_find(const int *cid, int q) {
 // mask. Returns the number of columns this lane's group added (leader only)
 // and counts the chunks it inserted into *new_chunks. tmask: the lanes of
 // this lane group (warp-level bit mask).
-template <int LOG2T>
+// GM selects how a chunk's lanes are grouped. The keys of one step are one B
+// row's columns, strictly increasing across the lanes that hold them (lanes
+// 0..len-1 of the group), so the lanes of a chunk are a contiguous run:
+//   GM 0: runs found from the left neighbour's chunk (shfl_up); the run's bits
+//         OR-ed by a segmented doubling scan of shfl_down;
+//   GM 1: runs as masks from a ballot of the run heads, bits OR-ed by one
+//         __reduce_or_sync over the run;
+//   GM 2: __match_any_sync on the chunk id (any order of keys).
+template <int LOG2T, int GM, int G>
 __device__ __forceinline__ int chunk_or(int *cid, unsigned *cmask, int key, unsigned tmask,
                                         int &new_chunks, int *err) {
-  const int q = key >= 0 ? (key >> 5) : -1;
-  const unsigned peers = __match_any_sync(tmask, q);
-  const unsigned bits = __reduce_or_sync(peers, key >= 0 ? 1u << (key & 31) : 0u);
   const int wl = threadIdx.x & 31;
-  if (q < 0 || wl != __ffs(peers) - 1) return 0;
+  const int gl = wl & (G - 1);  // lane inside the group
+  const unsigned bit = key >= 0 ? 1u << (key & 31) : 0u;
+  unsigned bits;
+  bool leader;
+  int q;
+  if constexpr (GM == 2) {
+    q = key >= 0 ? (key >> 5) : -1;
+    const unsigned peers = __match_any_sync(tmask, q);
+    bits = __reduce_or_sync(peers, bit);
+    leader = q >= 0 && wl == __ffs(peers) - 1;
+  } else {
+    q = key >= 0 ? (key >> 5) : -1 - gl;  // lanes without a key: distinct, never a chunk id
+    const int qp = __shfl_up_sync(tmask, q, 1, G);
+    const bool head = gl == 0 || qp != q;
+    leader = key >= 0 && head;
+    if constexpr (GM == 0) {
+      bits = bit;
+#pragma unroll
+      for (int d = 1; d < G; d <<= 1) {
+        const unsigned t = __shfl_down_sync(tmask, bits, d, G);
+        const int qn = __shfl_down_sync(tmask, q, d, G);
+        if (gl + d < G && qn == q) bits |= t;
+      }
+    } else {
+      const unsigned heads = __ballot_sync(tmask, head);
+      const unsigned upto = heads & (0xffffffffu >> (31 - wl));  // heads at or below this lane
+      const int first = 31 - __clz(upto);                         // this lane's run head
+      const unsigned above = heads & ~(0xffffffffu >> (31 - wl)); // heads above this lane
+      const unsigned gtop = tmask & ~(tmask >> 1) ? (tmask & ~(tmask >> 1)) : 0x80000000u;
+      const int last = above ? __ffs(above) - 2 : 31 - __clz(gtop);
+      const unsigned run = (0xffffffffu >> (31 - last)) & ~((1u << first) - 1u);
+      bits = __reduce_or_sync(run, bit);
+    }
+  }
+  if (!leader) return 0;
   int fresh = 0;
   const int s = chunk_slot<LOG2T>(cid, q, fresh, err);
   new_chunks += fresh;
@@ -115,7 +154,7 @@ struct SymChunkCfg {
   static constexpr int SMEM = GPC * BYTES;
 };
 
-template <int G, int LOG2T>
+template <int G, int LOG2T, int GM>
 __global__ void __launch_bounds__(256)
     k_sym_chunk(const int *__restrict__ arpt, const int *__restrict__ acol,
                 const int *__restrict__ brpt, const int *__restrict__ bcol,
@@ -161,14 +200,14 @@ __global__ void __launch_bounds__(256)
           const int e0 = q0.x + lane, e1 = q1.x + lane;
           const int k0 = e0 < q0.y ? __ldg(bcol + e0) : -1;
           const int k1 = e1 < q1.y ? __ldg(bcol + e1) : -1;
-          nz += chunk_or<LOG2T>(cid, cmask, k0, tmask, nch, err);
-          nz += chunk_or<LOG2T>(cid, cmask, k1, tmask, nch, err);
+          nz += chunk_or<LOG2T, GM, G>(cid, cmask, k0, tmask, nch, err);
+          nz += chunk_or<LOG2T, GM, G>(cid, cmask, k1, tmask, nch, err);
         } else {
           for (int i = 0; i < 2; ++i) {
             const int2 q = i ? q1 : q0;
             for (int e0 = q.x; e0 < q.y; e0 += G) {  // uniform trip count
               const int e = e0 + lane;
-              nz += chunk_or<LOG2T>(cid, cmask, e < q.y ? __ldg(bcol + e) : -1, tmask, nch, err);
+              nz += chunk_or<LOG2T, GM, G>(cid, cmask, e < q.y ? __ldg(bcol + e) : -1, tmask, nch, err);
             }
           }
         }
@@ -177,7 +216,7 @@ __global__ void __launch_bounds__(256)
         const int2 q = stage[t];
         for (int e0 = q.x; e0 < q.y; e0 += G) {
           const int e = e0 + lane;
-          nz += chunk_or<LOG2T>(cid, cmask, e < q.y ? __ldg(bcol + e) : -1, tmask, nch, err);
+          nz += chunk_or<LOG2T, GM, G>(cid, cmask, e < q.y ? __ldg(bcol + e) : -1, tmask, nch, err);
         }
       }
       tile.sync();  // stage reads done before the next chunk of A entries
@@ -195,40 +234,42 @@ __global__ void __launch_bounds__(256)
 
 template <int G, int LOG2T>
 static cudaError_t run_sym_chunk(const CsrDev &A, const CsrDev &B, const int *rows, int count,
-                                 int *row_nz, unsigned long long *chunks, int *err,
+                                 int *row_nz, unsigned long long *chunks, int *err, int gm,
                                  cudaStream_t s) {
   using C = SymChunkCfg<G, LOG2T>;
-  const void *f = (const void *)k_sym_chunk<G, LOG2T>;
-  const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
+  auto kern = gm == 2 ? k_sym_chunk<G, LOG2T, 2>
+            : gm == 1 ? k_sym_chunk<G, LOG2T, 1>
+                      : k_sym_chunk<G, LOG2T, 0>;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_chunk<G, LOG2T><<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, B.rpt, B.col, rows,
-                                                          count, row_nz, chunks, err);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, B.rpt, B.col, rows, count, row_nz,
+                                         chunks, err);
   return cudaGetLastError();
 }
 
 template <int G>
 static cudaError_t sym_chunk_bin(int bin, const CsrDev &A, const CsrDev &B, const int *rows,
                                  int count, int *row_nz, unsigned long long *chunks, int *err,
-                                 cudaStream_t s) {
+                                 int gm, cudaStream_t s) {
   switch (bin) {
-    case 0: return run_sym_chunk<G, 5>(A, B, rows, count, row_nz, chunks, err, s);
-    case 1: return run_sym_chunk<G, 6>(A, B, rows, count, row_nz, chunks, err, s);
-    case 2: return run_sym_chunk<G, 7>(A, B, rows, count, row_nz, chunks, err, s);
-    case 3: return run_sym_chunk<G, 8>(A, B, rows, count, row_nz, chunks, err, s);
-    case 4: return run_sym_chunk<G, 9>(A, B, rows, count, row_nz, chunks, err, s);
-    case 5: return run_sym_chunk<G, 10>(A, B, rows, count, row_nz, chunks, err, s);
-    case 6: return run_sym_chunk<G, 11>(A, B, rows, count, row_nz, chunks, err, s);
-    default: return run_sym_chunk<G, 12>(A, B, rows, count, row_nz, chunks, err, s);
+    case 0: return run_sym_chunk<G, 5>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    case 1: return run_sym_chunk<G, 6>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    case 2: return run_sym_chunk<G, 7>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    case 3: return run_sym_chunk<G, 8>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    case 4: return run_sym_chunk<G, 9>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    case 5: return run_sym_chunk<G, 10>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    case 6: return run_sym_chunk<G, 11>(A, B, rows, count, row_nz, chunks, err, gm, s);
+    default: return run_sym_chunk<G, 12>(A, B, rows, count, row_nz, chunks, err, gm, s);
   }
 }
 
-cudaError_t launch_symbolic_chunk(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+cudaError_t launch_symbolic_chunk(int bin, int lanes, int gm, const CsrDev &A, const CsrDev &B,
                                   const int *rows, int count, int *row_nz,
                                   unsigned long long *chunks, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  if (lanes == 8) return sym_chunk_bin<8>(bin, A, B, rows, count, row_nz, chunks, err, s);
-  if (lanes == 16) return sym_chunk_bin<16>(bin, A, B, rows, count, row_nz, chunks, err, s);
-  return sym_chunk_bin<32>(bin, A, B, rows, count, row_nz, chunks, err, s);
+  if (lanes == 8) return sym_chunk_bin<8>(bin, A, B, rows, count, row_nz, chunks, err, gm, s);
+  if (lanes == 16) return sym_chunk_bin<16>(bin, A, B, rows, count, row_nz, chunks, err, gm, s);
+  return sym_chunk_bin<32>(bin, A, B, rows, count, row_nz, chunks, err, gm, s);
 }
 
 // ---- numeric -----------------------------------------------------------------------
@@ -247,7 +288,7 @@ struct NumChunkCfg {
   static constexpr int SMEM = GPC * BYTES;
 };
 
-template <int G, int LOG2H, typename VT, int D>
+template <int G, int LOG2H, typename VT, int D, int GM>
 __global__ void __launch_bounds__(256)
     k_num_chunk(const int *__restrict__ arpt, const int *__restrict__ acol,
                 const VT *__restrict__ aval, const int *__restrict__ brpt,
@@ -308,7 +349,7 @@ __global__ void __launch_bounds__(256)
         const int4 q = stage[t];
         for (int e0 = q.x; e0 < q.y; e0 += G) {
           const int e = e0 + lane;
-          chunk_or<LOG2T>(cid, cmask, e < q.y ? __ldg(bcol + e) : -1, tmask, nch, err);
+          chunk_or<LOG2T, GM, G>(cid, cmask, e < q.y ? __ldg(bcol + e) : -1, tmask, nch, err);
         }
       }
       tile.sync();
@@ -481,11 +522,13 @@ __global__ void __launch_bounds__(256)
 template <int G, int LOG2H, typename VT>
 static cudaError_t run_num_chunk(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
                                  const int *crpt, int *ccol, double *cval, const int *rows,
-                                 int count, int *err, int depth, cudaStream_t s) {
+                                 int count, int *err, int depth, int gm, cudaStream_t s) {
   using C = NumChunkCfg<G, LOG2H>;
-  auto kern = depth >= 4 ? k_num_chunk<G, LOG2H, VT, 4>
-            : depth >= 2 ? k_num_chunk<G, LOG2H, VT, 2>
-                         : k_num_chunk<G, LOG2H, VT, 1>;
+  auto kern = gm == 2 ? k_num_chunk<G, LOG2H, VT, 2, 2>
+            : gm == 1 ? k_num_chunk<G, LOG2H, VT, 2, 1>
+            : depth >= 4 ? k_num_chunk<G, LOG2H, VT, 4, 0>
+            : depth >= 2 ? k_num_chunk<G, LOG2H, VT, 2, 0>
+                         : k_num_chunk<G, LOG2H, VT, 1, 0>;
   const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval,
@@ -494,11 +537,12 @@ static cudaError_t run_num_chunk(const CsrDev &A, const CsrDev &B, const VT *av,
 }
 
 template <int G>
-static cudaError_t num_chunk_bin(int bin, int depth, const CsrDev &A, const CsrDev &B,
+static cudaError_t num_chunk_bin(int bin, int depth, int gm, const CsrDev &A, const CsrDev &B,
                                  const int *crpt, int *ccol, double *cval, const int *rows,
                                  int count, int *err, cudaStream_t s) {
 #define NSPB_NCH(L2H) \
-  run_num_chunk<G, L2H, double>(A, B, A.val, B.val, crpt, ccol, cval, rows, count, err, depth, s)
+  run_num_chunk<G, L2H, double>(A, B, A.val, B.val, crpt, ccol, cval, rows, count, err, depth, \
+                                gm, s)
   switch (bin) {
     case 0: return NSPB_NCH(4);
     case 1: return NSPB_NCH(5);
@@ -510,14 +554,14 @@ static cudaError_t num_chunk_bin(int bin, int depth, const CsrDev &A, const CsrD
 #undef NSPB_NCH
 }
 
-cudaError_t launch_numeric_chunk(int bin, int lanes, int depth, const CsrDev &A,
+cudaError_t launch_numeric_chunk(int bin, int lanes, int depth, int gm, const CsrDev &A,
                                  const CsrDev &B, const int *crpt, int *ccol, double *cval,
                                  const int *rows, int count, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  if (lanes == 8) return num_chunk_bin<8>(bin, depth, A, B, crpt, ccol, cval, rows, count, err, s);
+  if (lanes == 8) return num_chunk_bin<8>(bin, depth, gm, A, B, crpt, ccol, cval, rows, count, err, s);
   if (lanes == 16)
-    return num_chunk_bin<16>(bin, depth, A, B, crpt, ccol, cval, rows, count, err, s);
-  return num_chunk_bin<32>(bin, depth, A, B, crpt, ccol, cval, rows, count, err, s);
+    return num_chunk_bin<16>(bin, depth, gm, A, B, crpt, ccol, cval, rows, count, err, s);
+  return num_chunk_bin<32>(bin, depth, gm, A, B, crpt, ccol, cval, rows, count, err, s);
 }
 
 }  // namespace nspb

@@ -130,11 +130,12 @@ cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth, co
 // ---- chunk.cu ---------------------------------------------------------------------
 // Row-group bins over column chunks (32 columns a chunk, a bit mask each).
 // Symbolic: *chunks receives the total number of chunks of the rows counted.
-// Numeric: fp64, B rows strictly increasing; depth as for the rowgroup kernels.
-cudaError_t launch_symbolic_chunk(int bin, int lanes, const CsrDev &A, const CsrDev &B,
+// Both need B rows strictly increasing; numeric is fp64; depth as for the
+// rowgroup kernels; gm picks how lanes of one chunk are grouped (see chunk.cu).
+cudaError_t launch_symbolic_chunk(int bin, int lanes, int gm, const CsrDev &A, const CsrDev &B,
                                   const int *rows, int count, int *row_nz,
                                   unsigned long long *chunks, int *err, cudaStream_t s);
-cudaError_t launch_numeric_chunk(int bin, int lanes, int depth, const CsrDev &A,
+cudaError_t launch_numeric_chunk(int bin, int lanes, int depth, int gm, const CsrDev &A,
                                  const CsrDev &B, const int *crpt, int *ccol, double *cval,
                                  const int *rows, int count, int *err, cudaStream_t s);
 

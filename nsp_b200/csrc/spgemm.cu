@@ -290,9 +290,9 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     const int c = h.sym_counts[b];
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
-    e = (b < kSymGroupBins && use_chunk())
-            ? launch_symbolic_chunk(b, lanes, A, B, rows, c, row_nz, &ctr->total_chunks,
-                                    &ctr->err, s)
+    e = (b < kSymGroupBins && b_sorted && use_chunk())
+            ? launch_symbolic_chunk(b, lanes, chunk_gm(), A, B, rows, c, row_nz,
+                                    &ctr->total_chunks, &ctr->err, s)
         : (b < kSymGroupBins && use_rg())
             ? launch_symbolic_rg(b, lanes, rg_depth(), A, B, rows, c, row_nz, &ctr->err, s)
             : launch_symbolic_bin(b, lanes, b_sorted, A, B, rows, c, row_nz, &ctr->err,
@@ -338,8 +338,8 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     int *ticket = &ctr->ticket[16 + b];
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
     if (b < kNumGroupBins && b_sorted && !comp && use_chunk()) {
-      e = launch_numeric_chunk(b, lanes, rg_depth(), A, B, crpt, ccol, cval, rows, c, &ctr->err,
-                               s);
+      e = launch_numeric_chunk(b, lanes, rg_depth(), chunk_gm(), A, B, crpt, ccol, cval, rows, c,
+                               &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;
       continue;

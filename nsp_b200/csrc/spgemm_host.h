@@ -71,7 +71,8 @@ struct Call {
   bool timing = false;
   // row-group bins through the rowgroup.cu kernels (opts.row_kernel 2 or 3)
   bool use_rg() const { return (opts.row_kernel & 0xff) == 2 || (opts.row_kernel & 0xff) == 3; }
-  bool use_chunk() const { return (opts.row_kernel & 0xff) == 4; }
+  bool use_chunk() const { int k = opts.row_kernel & 0xff; return k >= 4 && k <= 6; }
+  int chunk_gm() const { return (opts.row_kernel & 0xff) - 4; }
   // loads issued ahead in the row-group walks: bits 8.. of row_kernel (0 = 2)
   int rg_depth() const { return (opts.row_kernel >> 8) ? (opts.row_kernel >> 8) : 2; }
   void mark(int i) {
