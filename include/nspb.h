@@ -60,10 +60,14 @@ enum { NSPB_F64 = 0, NSPB_F32 = 1 };
 /* precision modes of the product */
 enum {
   NSPB_PREC_FP64 = 0,      /* fp64 inputs, fp64 accumulation (the drop-in)       */
-  NSPB_PREC_FP32_COMP = 1  /* fp32 inputs, error-free fp32 products and two-sum
+  NSPB_PREC_FP32_COMP = 1, /* fp32 inputs, error-free fp32 products and two-sum
                               compensated accumulation, fp64 output; rows whose
                               running error bound exceeds opts.comp_tol are
                               re-accumulated in fp64                            */
+  NSPB_PREC_FP32_WIDE = 2  /* fp32 inputs (half the value bytes), products
+                              exact in fp64 (24 + 24 significant bits), fp64
+                              accumulation in A-row order; |c - c*| <=
+                              n 2^-53 sum|a*b| for a row of n A entries         */
 };
 
 /* A CSR matrix on the device. rowptr has nrows+1 entries, 0-based, int32.   */
@@ -111,10 +115,14 @@ typedef struct {
   int32_t num_table_shift; /* 0: numeric row-group tables of twice the bin's
                             entry limit (load <= 1/2); 1: four times (load
                             <= 1/4); chosen by nspb_autotune              */
-  int32_t row_kernel;    /* row-group kernels: 0 = default, 1 = hash tables
-                            with an in-table bucket sort, 2 = staged walk with
-                            tables of four times the bin's row limit, 3 = the
-                            same with tables of twice the limit              */
+  int32_t row_kernel;    /* numeric row-group kernels (rows of <= 512 entries):
+                            0 = automatic: the staged walk when the rows
+                            compress (>= 1.5 intermediate products per entry
+                            of C), else hash tables with an in-table sort;
+                            1 = always the hash-sort kernels; 2 = always the
+                            staged walk (tables of 4x the bin's row limit);
+                            3 = staged walk with tables of 2x. Bits 8-15:
+                            B rows the staged walk loads ahead (0 = 4)       */
 } nspb_opts;
 
 /* Per-call figures (all optional; pass NULL).                               */

@@ -15,7 +15,7 @@ import ctypes as C
 import os
 
 from . import gen, matio
-from ._lib import (F32, F64, PREC_FP32_COMP, PREC_FP64, CsrIn, CsrOut, NspbError, Opts,
+from ._lib import (F32, F64, PREC_FP32_COMP, PREC_FP32_WIDE, PREC_FP64, CsrIn, CsrOut, NspbError, Opts,
                    SfCSR, Stats, check, lib)
 from .csr import DeviceCSR, HostCSR, adopt
 
@@ -30,6 +30,18 @@ def _stream_ptr(stream):
     if stream is None:
         stream = torch.cuda.current_stream()
     return C.c_void_p(stream.cuda_stream)
+
+
+def _precision(name: str) -> int:
+    """"fp64", "fp32c" (fp32 pairs, two-sum compensated) or "fp32w" (fp32
+    inputs, fp64 accumulation of exact products)."""
+    return {"fp64": PREC_FP64, "fp32c": PREC_FP32_COMP, "fp32w": PREC_FP32_WIDE}[precision_name(name)]
+
+
+def precision_name(name: str) -> str:
+    if name not in ("fp64", "fp32c", "fp32w"):
+        raise ValueError(f"precision {name!r}: expected fp64, fp32c or fp32w")
+    return name
 
 
 def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group_lanes=0,
@@ -67,7 +79,7 @@ def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR |
     With `out` given, its tensors are used as C's arrays (capacity = their
     length); otherwise the library allocates C (freed with the tensors)."""
     import torch
-    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    prec = _precision(precision)
     o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream, table_shift,
                   row_kernel)
     a, b = A.as_in(), B.as_in()
@@ -127,7 +139,7 @@ def autotune(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", reps: int = 3,
     """nspb_autotune: ({"group_lanes", "table_shift"} of the fastest candidate,
     [(group_lanes, table_shift, ms), ...] for every candidate)."""
     from ._lib import TuneEntry
-    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    prec = _precision(precision)
     o = make_opts(prec, stream=stream)
     best = Opts()
     rep = (TuneEntry * 6)()
@@ -153,7 +165,7 @@ def spgemm_host(A, B, out=None, nblocks: int = 0, precision: str = "fp64", strea
     of enough capacity C is written there; otherwise numpy arrays are sized by
     a first call. Returns (rowptr, col, val)."""
     import numpy as np
-    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    prec = _precision(precision)
     o = make_opts(prec, stream=stream)
 
     def host_in(M):
@@ -201,7 +213,7 @@ class Plan:
                  max_group: int = 0):
         import torch
         m = len(As)
-        prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+        prec = _precision(precision)
         o = make_opts(prec, False, check_errors, 0, 1e-10, stream)
         o.batch_max_products = int(max_group)
         a = (CsrIn * m)(*[x.as_in() for x in As])
@@ -239,7 +251,7 @@ def spgemm_batched(As, Bs, precision: str = "fp64", stream=None, return_stats: b
     tensors view the shared output allocations (freed with the last view)."""
     import torch
     m = len(As)
-    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    prec = _precision(precision)
     o = make_opts(prec, False, True, 0, 1e-10, stream)
     o.batch_max_products = int(max_group)
     a = (CsrIn * m)(*[x.as_in() for x in As])
@@ -301,7 +313,7 @@ def spgemm_numeric(A: DeviceCSR, B: DeviceCSR, rowptr, nnz: int, precision="fp64
                    stream=None, assume_sorted=False) -> DeviceCSR:
     """Two-call form, step 2: fills col/val for the given rowptr."""
     import torch
-    prec = PREC_FP32_COMP if precision == "fp32c" else PREC_FP64
+    prec = _precision(precision)
     o = make_opts(prec, assume_sorted, True, 0, 1e-12, stream)
     a, b = A.as_in(), B.as_in()
     col = torch.empty(max(nnz, 1), dtype=torch.int32, device=rowptr.device)

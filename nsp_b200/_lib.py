@@ -35,6 +35,7 @@ F64 = 0
 F32 = 1
 PREC_FP64 = 0
 PREC_FP32_COMP = 1
+PREC_FP32_WIDE = 2
 
 
 class CsrIn(C.Structure):

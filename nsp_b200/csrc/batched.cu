@@ -280,7 +280,7 @@ static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, 
                          const nspb_opts &o, nspb_stats *stats, void **owners, int *n_owners) {
   cudaStream_t s = static_cast<cudaStream_t>(o.stream);
   CatHost h;
-  int st = cat_layout(count, A, B, o.precision == NSPB_PREC_FP32_COMP, h);
+  int st = cat_layout(count, A, B, fp32_inputs(o.precision), h);
   if (st) return st;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -508,7 +508,7 @@ int group_create(int count, const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr
   int st;
   nspb_csr_in a = A[0], b = B[0];
   if (G->cat) {
-    if ((st = cat_layout(count, A, B, o.precision == NSPB_PREC_FP32_COMP, G->h))) return st;
+    if ((st = cat_layout(count, A, B, fp32_inputs(o.precision), G->h))) return st;
     if ((st = dev_alloc(&G->ws_cat, G->h.bytes))) return st;
     std::vector<char> host;
     cudaError_t e = cat_build(G->h, G->ws_cat, host, s);

@@ -30,6 +30,11 @@ struct CsrDev {
 // Flag bits written by launch_check_sorted.
 enum : int { B_UNSORTED = 1 };
 
+// fp32 input modes (compensated pairs, or fp64 accumulation of exact products).
+inline bool fp32_inputs(int precision) {
+  return precision == NSPB_PREC_FP32_COMP || precision == NSPB_PREC_FP32_WIDE;
+}
+
 // Compensated-mode parameters of a numeric launch (fp32 inputs).
 struct CompArgs {
   int nmax;        // rows with at most nmax A entries accumulate error-free in
@@ -111,13 +116,11 @@ cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorte
                                     int *ticket, int tshift, cudaStream_t s);
 
 // ---- rowgroup.cu ----------------------------------------------------------------
-// Row-group bins (symbolic bins < kSymGroupBins, numeric bins < kNumGroupBins)
-// with lane groups of `lanes` lanes. Numeric: B rows strictly increasing;
-// tshift 0 gives tables of four times the bin's row limit, -1 twice. depth:
-// B rows whose loads are issued together before their inserts (1, 2, 4, 8).
-cudaError_t launch_symbolic_rg(int bin, int lanes, int depth, const CsrDev &A, const CsrDev &B,
-                               const int *rows, int count, int *row_nz, int *err,
-                               cudaStream_t s);
+// Staged-walk numeric kernels of the row-group bins (numeric bins <
+// kNumGroupBins) with lane groups of `lanes` lanes; B rows strictly
+// increasing. tshift 0 gives tables of four times the bin's row limit, -1
+// twice. depth: B rows whose loads are issued together before their inserts
+// (1, 2 or 4).
 cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
                               const CsrDev &B,
                               const int *crpt, int *ccol, double *cval, const int *rows,
@@ -126,17 +129,5 @@ cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth, co
                                    const CsrDev &B, const int *crpt, int *ccol, double *cval,
                                    const int *rows, int count, int nmax, int *redo, int *max_deg,
                                    int *err, cudaStream_t s);
-
-// ---- chunk.cu ---------------------------------------------------------------------
-// Row-group bins over column chunks (32 columns a chunk, a bit mask each).
-// Symbolic: *chunks receives the total number of chunks of the rows counted.
-// Both need B rows strictly increasing; numeric is fp64; depth as for the
-// rowgroup kernels; gm picks how lanes of one chunk are grouped (see chunk.cu).
-cudaError_t launch_symbolic_chunk(int bin, int lanes, int gm, const CsrDev &A, const CsrDev &B,
-                                  const int *rows, int count, int *row_nz,
-                                  unsigned long long *chunks, int *err, cudaStream_t s);
-cudaError_t launch_numeric_chunk(int bin, int lanes, int depth, int gm, const CsrDev &A,
-                                 const CsrDev &B, const int *crpt, int *ccol, double *cval,
-                                 const int *rows, int count, int *err, cudaStream_t s);
 
 }  // namespace nspb

@@ -1,27 +1,32 @@
-// Row-group kernels of both phases: rows whose intermediate products
-// (symbolic) or entries (numeric) fit one lane group's shared-memory table.
-// These rows carry nearly all the work of stencil, AMG and random products.
+// Staged-walk numeric kernels of the row-group bins: rows of at most 512
+// entries whose B rows are strictly increasing, one lane group a row. The
+// host takes them when the rows compress (at least 1.5 intermediate products
+// per entry of C); otherwise numeric.cu's hash-sort kernels run.
 //
 // Reference counterparts (amavliut/nsp, nsp/src/nsp.cu):
-//   nsp_set_row_nz_bin_mpwarp / _each_tb            :477-586 (symbolic)
-//   nsp_calculate_value_col_bin_mpwarp / _each_warp :1307-1494 (numeric, with
-//                                                   the O(nnz^2) rank sort)
+//   nsp_calculate_value_col_bin_mpwarp / _each_warp :1307-1494 (shared-memory
+//   hash with atomic adds, then an O(nnz^2) rank sort)
 //
 // Shape of one row (a lane group of G lanes, G = 8, 16 or 32):
 //   - the A row is taken G entries at a time; each lane stages one entry's
 //     {B row start, B row end, A value} in shared memory, so every step reads
 //     its B row bounds with one broadcast load;
+//   - D B rows at a time have their columns and values loaded before the
+//     first of them is inserted (loads in flight while the table is updated);
 //   - a step covers one B row, a lane per entry; its key is looked up at its
 //     home slot first, and only a miss enters the probe loop (a 4x-load table
 //     makes almost every step of a stencil row collision-free);
-//   - numeric: values are not cleared between rows; the lane that inserts a
-//     key writes 0 + a*b, later steps add in A-row order (deterministic, bit
-//     for bit the oracle's sum);
-//   - numeric: the row is sorted by a bucket counting sort whose monotone map
-//     spans [first column, last column] of the row, taken from the ends of
-//     the (sorted) B rows while staging; the compaction of the table counts
-//     the buckets as it goes, and every entry is stored straight to its rank
-//     in C (no sorted copy in shared memory).
+//   - values are not cleared between rows; the lane that inserts a key writes
+//     0 + a*b, later steps add in A-row order (deterministic, bit for bit the
+//     oracle's sum);
+//   - the row is sorted by a bucket counting sort whose monotone map spans
+//     [first column, last column] of the row, taken from the ends of the
+//     (sorted) B rows while staging; the compaction of the table counts the
+//     buckets as it goes, and every entry is stored straight to its rank in C
+//     (no sorted copy in shared memory).
+// These kernels, like the hash-sort ones, are bound by the shared-memory data
+// pipe (ncu on the 80^3 stencil: L1 data-pipe wavefronts 88% of peak, 32 a B
+// row step, 42% of them bank conflicts), not by instruction issue or DRAM.
 #include "common.cuh"
 #include "internal.h"
 #include "launch_util.h"
@@ -69,136 +74,6 @@ __device__ __forceinline__ unsigned rg_bucket_mul(unsigned span, int nb) {
 }
 __device__ __forceinline__ int rg_bucket(int key, int lo, unsigned mul) {
   return (int)__umulhi((unsigned)key - (unsigned)lo, mul);
-}
-
-// ---- symbolic --------------------------------------------------------------------
-template <int G, int LOG2T>
-struct SymRgCfg {
-  static constexpr int T = 1 << LOG2T;
-  static constexpr int BYTES = T * 4 + G * 8;
-  static constexpr int kBySmem = (48 * 1024) / BYTES > 0 ? (48 * 1024) / BYTES : 1;
-  static constexpr int GPC = kBySmem < 256 / G ? kBySmem : 256 / G;
-  static constexpr int THREADS = GPC * G;
-  static constexpr int SMEM = GPC * BYTES;
-};
-
-template <int G, int LOG2T, int D>
-__global__ void __launch_bounds__(256)
-    k_sym_rg(const int *__restrict__ arpt, const int *__restrict__ acol,
-             const int *__restrict__ brpt, const int *__restrict__ bcol,
-             const int *__restrict__ rows, int count, int *__restrict__ row_nz,
-             int *__restrict__ err) {
-  using C = SymRgCfg<G, LOG2T>;
-  extern __shared__ __align__(16) unsigned char smem_srg[];
-  auto tile = cg::tiled_partition<G>(cg::this_thread_block());
-  const int g = threadIdx.x / G;
-  const int lane = tile.thread_rank();
-  int *table = reinterpret_cast<int *>(smem_srg + (size_t)g * C::BYTES);
-  int2 *stage = reinterpret_cast<int2 *>(table + C::T);
-  int4 *t4 = reinterpret_cast<int4 *>(table);
-#pragma unroll 4
-  for (int s = lane; s < C::T / 4; s += G) t4[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
-  tile.sync();
-  auto insert = [&](int key) -> int {
-    bool fresh;
-    rg_slot<LOG2T>(table, key, fresh, err);
-    return fresh ? 1 : 0;
-  };
-  for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
-    const int row = rows ? rows[r] : r;
-    const int a0 = arpt[row], a1 = arpt[row + 1];
-    int nz = 0;
-    for (int ab = a0; ab < a1; ab += G) {
-      const int j = ab + lane;
-      if (j < a1) {
-        const int k = ld_stream(acol + j);
-        stage[lane] = make_int2(__ldg(brpt + k), __ldg(brpt + k + 1));
-      }
-      tile.sync();
-      const int na = min(G, a1 - ab);
-      int t = 0;
-      // D B rows a round: every row's keys are loaded before any is inserted
-      for (; t + D <= na; t += D) {
-        int2 q[D];
-        bool shortrows = true;
-#pragma unroll
-        for (int i = 0; i < D; ++i) {
-          q[i] = stage[t + i];
-          shortrows &= q[i].y - q[i].x <= G;
-        }
-        if (shortrows) {
-          int k[D];
-#pragma unroll
-          for (int i = 0; i < D; ++i) {
-            const int e = q[i].x + lane;
-            k[i] = e < q[i].y ? __ldg(bcol + e) : -1;
-          }
-#pragma unroll
-          for (int i = 0; i < D; ++i)
-            if (k[i] >= 0) nz += insert(k[i]);
-        } else {
-#pragma unroll 1
-          for (int i = 0; i < D; ++i)
-            for (int e = q[i].x + lane; e < q[i].y; e += G) nz += insert(__ldg(bcol + e));
-        }
-      }
-      for (; t < na; ++t) {
-        const int2 q = stage[t];
-        for (int e = q.x + lane; e < q.y; e += G) nz += insert(__ldg(bcol + e));
-      }
-      tile.sync();  // stage reads done before the next chunk rewrites it
-    }
-    nz = cg::reduce(tile, nz, cg::plus<int>());
-    if (lane == 0) row_nz[row] = nz;
-#pragma unroll 4
-    for (int s = lane; s < C::T / 4; s += G) t4[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
-    tile.sync();
-  }
-}
-
-template <int G, int LOG2T, int D>
-static cudaError_t run_sym_rg(const CsrDev &A, const CsrDev &B, const int *rows, int count,
-                              int *row_nz, int *err, cudaStream_t s) {
-  using C = SymRgCfg<G, LOG2T>;
-  const void *f = (const void *)k_sym_rg<G, LOG2T, D>;
-  const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
-  if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_rg<G, LOG2T, D><<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, B.rpt, B.col, rows,
-                                                          count, row_nz, err);
-  return cudaGetLastError();
-}
-
-template <int G, int D>
-static cudaError_t sym_rg_bin(int bin, const CsrDev &A, const CsrDev &B, const int *rows,
-                              int count, int *row_nz, int *err, cudaStream_t s) {
-  switch (bin) {
-    case 0: return run_sym_rg<G, 5, D>(A, B, rows, count, row_nz, err, s);
-    case 1: return run_sym_rg<G, 6, D>(A, B, rows, count, row_nz, err, s);
-    case 2: return run_sym_rg<G, 7, D>(A, B, rows, count, row_nz, err, s);
-    case 3: return run_sym_rg<G, 8, D>(A, B, rows, count, row_nz, err, s);
-    case 4: return run_sym_rg<G, 9, D>(A, B, rows, count, row_nz, err, s);
-    case 5: return run_sym_rg<G, 10, D>(A, B, rows, count, row_nz, err, s);
-    case 6: return run_sym_rg<G, 11, D>(A, B, rows, count, row_nz, err, s);
-    default: return run_sym_rg<G, 12, D>(A, B, rows, count, row_nz, err, s);
-  }
-}
-
-template <int D>
-static cudaError_t sym_rg_lanes(int bin, int lanes, const CsrDev &A, const CsrDev &B,
-                                const int *rows, int count, int *row_nz, int *err,
-                                cudaStream_t s) {
-  if (lanes == 8) return sym_rg_bin<8, D>(bin, A, B, rows, count, row_nz, err, s);
-  if (lanes == 16) return sym_rg_bin<16, D>(bin, A, B, rows, count, row_nz, err, s);
-  return sym_rg_bin<32, D>(bin, A, B, rows, count, row_nz, err, s);
-}
-
-cudaError_t launch_symbolic_rg(int bin, int lanes, int depth, const CsrDev &A, const CsrDev &B,
-                               const int *rows, int count, int *row_nz, int *err,
-                               cudaStream_t s) {
-  if (count <= 0) return cudaSuccess;
-  if (depth >= 8) return sym_rg_lanes<8>(bin, lanes, A, B, rows, count, row_nz, err, s);
-  if (depth >= 4) return sym_rg_lanes<4>(bin, lanes, A, B, rows, count, row_nz, err, s);
-  return sym_rg_lanes<2>(bin, lanes, A, B, rows, count, row_nz, err, s);
 }
 
 // ---- numeric ---------------------------------------------------------------------

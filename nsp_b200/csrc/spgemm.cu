@@ -104,11 +104,12 @@ HostStage *host_stage() {
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // Lanes per row group from the mean length of the B rows the products read.
-// Measured with the autotuner on B200: 32 lanes win from a mean of 8 entries up
-// (random, AMG and stencil products); 8 lanes only for B rows of about 4
-// entries when A has enough rows to fill the GPU with the smaller groups.
+// Measured on B200: 32 lanes win from a mean of 8 entries up (random, AMG and
+// stencil products); 8 lanes below that when A has enough rows to fill the GPU
+// with the smaller groups (7-point Laplacian 128^3, mean 6.9: 2.7 ms with 8
+// lanes, 4.7 ms with 32).
 static int pick_lanes(double mean_b_row, int a_rows) {
-  return (mean_b_row <= 6.0 && a_rows >= 65536) ? 8 : 32;
+  return (mean_b_row < 7.5 && a_rows >= 65536) ? 8 : 32;
 }
 
 // ---- a call --------------------------------------------------------------------
@@ -123,9 +124,8 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   if ((a->nrows > 0 && !a->rowptr) || (b->nrows > 0 && !b->rowptr)) return NSPB_ERR_INVALID;
   if ((a->nnz > 0 && (!a->col || !a->val)) || (b->nnz > 0 && (!b->col || !b->val)))
     return NSPB_ERR_INVALID;
-  const int want = opts.precision == NSPB_PREC_FP32_COMP ? NSPB_F32 : NSPB_F64;
-  if (opts.precision != NSPB_PREC_FP64 && opts.precision != NSPB_PREC_FP32_COMP)
-    return NSPB_ERR_INVALID;
+  const int want = fp32_inputs(opts.precision) ? NSPB_F32 : NSPB_F64;
+  if (opts.precision != NSPB_PREC_FP64 && !fp32_inputs(opts.precision)) return NSPB_ERR_INVALID;
   if ((a->nnz > 0 && a->val_type != want) || (b->nnz > 0 && b->val_type != want))
     return NSPB_ERR_INVALID;
   int ndev = 0;
@@ -290,13 +290,8 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     const int c = h.sym_counts[b];
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
-    e = (b < kSymGroupBins && b_sorted && use_chunk())
-            ? launch_symbolic_chunk(b, lanes, chunk_gm(), A, B, rows, c, row_nz,
-                                    &ctr->total_chunks, &ctr->err, s)
-        : (b < kSymGroupBins && use_rg())
-            ? launch_symbolic_rg(b, lanes, rg_depth(), A, B, rows, c, row_nz, &ctr->err, s)
-            : launch_symbolic_bin(b, lanes, b_sorted, A, B, rows, c, row_nz, &ctr->err,
-                                  &ctr->ticket[b], s);
+    e = launch_symbolic_bin(b, lanes, b_sorted, A, B, rows, c, row_nz, &ctr->err,
+                            &ctr->ticket[b], s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
@@ -329,23 +324,19 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     if ((e = order_block_bins(crpt, 1, h.num_counts, kNumGroupBins, kNumBins, off)) != cudaSuccess)
       return cuda_fail(e);
   }
-  const bool comp = opts.precision == NSPB_PREC_FP32_COMP;
-  const int nmax = comp ? comp_nmax(opts.comp_tol) : 0;
+  // fp32 inputs: rows of at most nmax A entries accumulate in fp32 pairs, the
+  // others (every row in the wide mode) in fp64 from exact products
+  const bool comp = fp32_inputs(opts.precision);
+  const int nmax = opts.precision == NSPB_PREC_FP32_COMP ? comp_nmax(opts.comp_tol) : 0;
+  const bool staged = use_staged();
   for (int b = 0; b < kNumBins; ++b) {
     const int c = h.num_counts[b];
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
     int *ticket = &ctr->ticket[16 + b];
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
-    if (b < kNumGroupBins && b_sorted && !comp && use_chunk()) {
-      e = launch_numeric_chunk(b, lanes, rg_depth(), chunk_gm(), A, B, crpt, ccol, cval, rows, c,
-                               &ctr->err, s);
-      if (e != cudaSuccess) return cuda_fail(e);
-      ++launches;
-      continue;
-    }
-    if (b < kNumGroupBins && b_sorted && (use_rg() || (comp && use_chunk()))) {
-      const int rg_shift = (opts.row_kernel & 0xff) == 3 ? -1 : 0;
+    if (b < kNumGroupBins && b_sorted && staged) {
+      const int rg_shift = (opts.row_kernel & 0xff) == 3 ? -1 : 0;  // tables 2x, else 4x
       e = comp ? launch_numeric_comp_rg(b, lanes, rg_shift, rg_depth(), A, B, crpt, ccol, cval, rows, c, nmax,
                                         &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
                : launch_numeric_rg(b, lanes, rg_shift, rg_depth(), A, B, crpt, ccol, cval, rows, c,

@@ -26,7 +26,6 @@ struct DevCounters {
   int max_comp_deg;  // compensated mode: largest A-row degree of a pair row
   int long_rows;     // rows listed for the block-per-row intermediate-product count
   int pad;
-  unsigned long long total_chunks;  // column chunks of the rows the chunk kernels counted
   int ticket[32];    // row tickets of the block-per-row launches (symbolic
                      // bin b at b, numeric bin b at 16 + b)
 };
@@ -69,12 +68,20 @@ struct Call {
   // opts.timing: events around rowinfo, symbolic, scan, numeric
   cudaEvent_t ev[8] = {};
   bool timing = false;
-  // row-group bins through the rowgroup.cu kernels (opts.row_kernel 2 or 3)
-  bool use_rg() const { return (opts.row_kernel & 0xff) == 2 || (opts.row_kernel & 0xff) == 3; }
-  bool use_chunk() const { int k = opts.row_kernel & 0xff; return k >= 4 && k <= 6; }
-  int chunk_gm() const { return (opts.row_kernel & 0xff) - 4; }
-  // loads issued ahead in the row-group walks: bits 8.. of row_kernel (0 = 2)
-  int rg_depth() const { return (opts.row_kernel >> 8) ? (opts.row_kernel >> 8) : 2; }
+  // Numeric row-group bins through the staged-walk kernels (rowgroup.cu)?
+  // opts.row_kernel 2 or 3 always, 1 never, 0 when the rows compress: at
+  // least 1.5 intermediate products per entry of C (measured on B200: the
+  // staged walk wins on stencils, 1.04x, and 7-point Laplacians, 1.27x, and
+  // loses on random and power-law rows, where almost every product is a new
+  // entry). Needs B rows strictly increasing.
+  bool use_staged() const {
+    const int k = opts.row_kernel & 0xff;
+    if (k == 2 || k == 3) return true;
+    if (k != 0) return false;
+    return h.total_nnz > 0 && (double)intprod >= 1.5 * (double)h.total_nnz;
+  }
+  // B rows whose loads the staged walk issues ahead: bits 8.. of row_kernel (0 = 4)
+  int rg_depth() const { return (opts.row_kernel >> 8) ? (opts.row_kernel >> 8) : 4; }
   void mark(int i) {
     if (timing && ev[i]) cudaEventRecord(ev[i], s);
   }

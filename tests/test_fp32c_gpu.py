@@ -67,3 +67,31 @@ def test_fp32c_rejects_fp64_inputs(cuda):
     A = nb.gen.stencil(5, npts=27).to_device()
     with pytest.raises(nb.NspbError):
         nb.spgemm(A, A, precision="fp32c")
+
+
+@pytest.mark.parametrize("case", ["stencil27", "random"])
+def test_fp32w_is_exact_fp64_accumulation(cuda, case):
+    """fp32 inputs with fp64 accumulation: every product of two fp32 values is
+    exact in fp64, so the result equals the fp64 oracle on the widened values
+    bit for bit (row-group path), within 1e-12 of sum|ab| everywhere."""
+    if case == "stencil27":
+        A = B = nb.gen.stencil(16, npts=27, fp32=True)
+    else:
+        A = nb.gen.random(3000, 2500, 1, 30, seed=4, fp32=True)
+        B = nb.gen.random(2500, 4000, 1, 40, seed=5, fp32=True)
+    C, st = nb.spgemm(as32(A).to_device(), as32(B).to_device(), precision="fp32w",
+                      return_stats=True)
+    got = C.to_host()
+    rp, col, val = oracle.spgemm(A, B)
+    assert_same_structure(got.rowptr, got.col, rp, col)
+    if sum(st["num_bins"][6:]) == 0:
+        assert_bitwise(got.val, val)
+    else:
+        assert_close(got.val, val, oracle.absbound(A, B, rp, col))
+
+
+def test_fp32w_rejects_fp64_inputs(cuda):
+    A = nb.gen.stencil(5, npts=27).to_device()
+    with pytest.raises(nb.NspbError):
+        nb.spgemm(A, A, precision="fp32w")
+

@@ -93,12 +93,15 @@ def _fp32c_check(A, label):
     assert_close(h.val, val, bound, tol=1e-10)
     err = np.abs(h.val - val)
     scaled = float(np.max(err / np.maximum(bound, 1e-300)))
-    away = np.abs(val) > 1e-8 * bound
+    # per-entry relative error away from cancellation: the Dot2 bound is
+    # relative to sum|ab|, so an entry that cancels to 1e-6 of its sum|ab|
+    # can carry 1e-6 relative error at 1e-12 scaled error
+    away = np.abs(val) > 1e-3 * bound
     rel = float(np.max(err[away] / np.abs(val[away]))) if away.any() else 0.0
     print(f"{label} fp32c vs fp64 oracle: max |c-c*|/sum|ab| {scaled:.3e}, max relative "
-          f"error {rel:.3e} over {int(away.sum())} of {len(val)} entries (|c*| > 1e-8 sum|ab|), "
+          f"error {rel:.3e} over {int(away.sum())} of {len(val)} entries (|c*| > 1e-3 sum|ab|), "
           f"a-priori bound {st['max_row_err']:.3e}, rows in fp64 {st['rows_redone']}")
-    assert rel <= 1e-10
+    assert scaled <= 1e-10 and rel <= 1e-10
     return st
 
 
