@@ -3,15 +3,14 @@
 // The reference has no batched entry: an AMG setup calls the product once per
 // Galerkin step from the host (src/spspmpi.cu:266-313 per call), each call
 // creating streams, allocating scratch and synchronising 4-6 times. Here the
-// batch is one block-diagonal product:
-//   A_cat = diag(A[0], ..., A[m-1]),  B_cat = diag(B[0], ..., B[m-1])
-//   C_cat = A_cat·B_cat = diag(A[0]B[0], ..., A[m-1]B[m-1])
-// One kernel copies the operands into the block-diagonal layout (columns of
-// A[p] shifted by the first row of B[p] in B_cat, columns of B[p] by its first
-// column), the standard pipeline then runs once over all rows of all
-// products (one launch per phase and bin; the bins form a single work queue
-// across products; two host synchronisations in total), and one kernel
-// splits C_cat back into per-product row pointers and columns.
+// rows of all products form one row space (product p owns the global rows
+// [row_off[p], row_off[p+1])), and every phase runs once over it: one launch
+// per phase and bin, the bins a single work queue across products, two host
+// synchronisations in total. The kernels read each row's operands through a
+// device table of per-product descriptors (A's and B's arrays where they lie,
+// B's column count) and a row-to-product map, so no operand is copied; C is
+// written into one allocation per group, each product's C a view of it, with
+// per-product row pointers taken from the group's row pointer.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,59 +24,27 @@
 
 namespace nspb {
 
-struct CatDesc {
-  const int *rpt;
-  const int *col;
-  const void *val;
-  long long row_off;  // first row of this block in the concatenation
-  long long nnz_off;  // first entry of this block
-  int nrows;
-  int col_shift;      // added to every column of this block
-};
-
-// The concatenation and split kernels run on a 2-D grid: blockIdx.y is the
-// product, blockIdx.x strides over that product's rows or entries, so no item
-// has to search for its product.
-template <typename VT>
-__global__ void k_cat_entries(const CatDesc *__restrict__ d, int *__restrict__ col,
-                              VT *__restrict__ val) {
-  const CatDesc q = d[blockIdx.y];
-  const long long n = (long long)(q.nrows > 0 ? q.rpt[q.nrows] - q.rpt[0] : 0);
-  const long long e0 = q.nrows > 0 ? q.rpt[0] : 0;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    col[q.nnz_off + e] = q.col[e0 + e] + q.col_shift;
-    val[q.nnz_off + e] = static_cast<const VT *>(q.val)[e0 + e];
-  }
-}
-
-__global__ void k_cat_rows(const CatDesc *__restrict__ d, long long total, long long nnz_total,
-                           int *__restrict__ rpt) {
-  const CatDesc q = d[blockIdx.y];
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < q.nrows;
-       i += (long long)gridDim.x * blockDim.x)
-    rpt[q.row_off + i] = (int)(q.nnz_off + (q.rpt[i] - q.rpt[0]));
-  if (blockIdx.y == 0 && blockIdx.x == 0 && threadIdx.x == 0) rpt[total] = (int)nnz_total;
-}
-
-// Per-product row pointers (product p's at out_rpt + row_off[p] + p) and the
-// column shift undone in place.
-__global__ void k_split(const int *__restrict__ crpt, const long long *__restrict__ row_off,
-                        const int *__restrict__ shift, int *__restrict__ out_rpt,
-                        int *__restrict__ ccol) {
+// The product of every global row: blockIdx.y is the product.
+__global__ void k_fill_rows(const int *__restrict__ row_off, int *__restrict__ prod_of_row) {
   const int p = blockIdx.y;
-  const long long r0 = row_off[p], n = row_off[p + 1] - r0;
-  const int c0 = crpt[r0], c1 = crpt[r0 + n], sh = shift[p];
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
-       i += (long long)gridDim.x * blockDim.x)
+  const int r0 = row_off[p], r1 = row_off[p + 1];
+  for (int r = r0 + blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += gridDim.x * blockDim.x)
+    prod_of_row[r] = p;
+}
+
+// Per-product row pointers (product p's at out_rpt + row_off[p] + p) from the
+// group's row pointer.
+__global__ void k_split_rows(const int *__restrict__ crpt, const int *__restrict__ row_off,
+                             int *__restrict__ out_rpt) {
+  const int p = blockIdx.y;
+  const int r0 = row_off[p], n = row_off[p + 1] - r0;
+  const int c0 = crpt[r0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
     out_rpt[r0 + p + i] = crpt[r0 + i] - c0;
-  for (long long t = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; t < c1;
-       t += (long long)gridDim.x * blockDim.x)
-    ccol[t] -= sh;
 }
 
 // starts[p] = crpt[row_off[p]] for p <= m (row_off[m] = all rows).
-__global__ void k_gather_starts(const int *__restrict__ crpt, const long long *__restrict__ row_off,
+__global__ void k_gather_starts(const int *__restrict__ crpt, const int *__restrict__ row_off,
                                 int m, int *__restrict__ starts) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= m; p += gridDim.x * blockDim.x)
     starts[p] = crpt[row_off[p]];
@@ -101,196 +68,149 @@ static int grid_cap(long long n) {
 
 using namespace nspb;
 
-// Host-side layout of the block-diagonal operands of `count` products and the
-// offsets of one device block holding descriptors, offsets, the concatenated
-// A and B and C_cat's row pointer.
-struct CatHost {
+// Host-side description of one group's product table and the offsets of one
+// device block holding it: the per-product operands, each product's first
+// global row, the product of every global row, the group's row pointer and
+// the per-product starts in C.
+struct TableHost {
   int count = 0;
   bool f32 = false;
-  long long rows_a = 0, rows_b = 0, cols_b = 0, nnz_a = 0, nnz_b = 0;
-  long long max_ra = 0, max_rb = 0, max_na = 0, max_nb = 0;
-  std::vector<CatDesc> da, db;
-  std::vector<long long> a_rows, a_nnz, b_rows, b_nnz;
-  std::vector<int> cshift;
-  size_t o_da, o_db, o_ar, o_an, o_br, o_bn, o_sh, o_arp, o_acl, o_avl, o_brp, o_bcl, o_bvl,
-      o_crp, o_st, bytes;
+  long long rows = 0, a_nnz = 0, max_rows = 0;
+  int max_ncols = 0, max_brows = 0;
+  std::vector<Operands<double>> ops;  // value pointers of fp32 operands stored as-is
+  std::vector<int> row_off;
+  size_t o_ops = 0, o_roff = 0, o_por = 0, o_crp = 0, o_st = 0, bytes = 0;
 };
 
-static int cat_layout(int count, const nspb_csr_in *A, const nspb_csr_in *B, bool f32,
-                      CatHost &h) {
+static int table_layout(int count, const nspb_csr_in *A, const nspb_csr_in *B, bool f32,
+                        TableHost &h) {
   h.count = count;
   h.f32 = f32;
-  h.da.resize(count);
-  h.db.resize(count);
-  h.a_rows.resize(count + 1);
-  h.a_nnz.resize(count + 1);
-  h.b_rows.resize(count + 1);
-  h.b_nnz.resize(count + 1);
-  h.cshift.resize(count);
+  h.ops.resize(count);
+  h.row_off.resize(count + 1);
   for (int p = 0; p < count; ++p) {
     const nspb_csr_in &a = A[p], &b = B[p];
     if (a.nrows < 0 || a.ncols != b.nrows || b.ncols < 0 || a.nnz < 0 || b.nnz < 0 ||
         (a.nrows > 0 && !a.rowptr) || (b.nrows > 0 && !b.rowptr) ||
         (a.nnz > 0 && (!a.col || !a.val)) || (b.nnz > 0 && (!b.col || !b.val)))
       return NSPB_ERR_INVALID;
+    if (a.nnz > INT32_MAX || b.nnz > INT32_MAX) return NSPB_ERR_INVALID;
     if ((a.nnz > 0 && a.val_type != (f32 ? NSPB_F32 : NSPB_F64)) ||
         (b.nnz > 0 && b.val_type != (f32 ? NSPB_F32 : NSPB_F64)))
       return NSPB_ERR_INVALID;
-    h.da[p] = CatDesc{a.rowptr, a.col, a.val, h.rows_a, h.nnz_a, a.nrows, (int)h.rows_b};
-    h.db[p] = CatDesc{b.rowptr, b.col, b.val, h.rows_b, h.nnz_b, b.nrows, (int)h.cols_b};
-    h.cshift[p] = (int)h.cols_b;
-    h.a_rows[p] = h.rows_a;
-    h.a_nnz[p] = h.nnz_a;
-    h.b_rows[p] = h.rows_b;
-    h.b_nnz[p] = h.nnz_b;
-    h.rows_a += a.nrows;
-    h.nnz_a += a.nnz;
-    h.rows_b += b.nrows;
-    h.nnz_b += b.nnz;
-    h.cols_b += b.ncols;
-    h.max_ra = std::max<long long>(h.max_ra, a.nrows);
-    h.max_rb = std::max<long long>(h.max_rb, b.nrows);
-    h.max_na = std::max<long long>(h.max_na, a.nnz);
-    h.max_nb = std::max<long long>(h.max_nb, b.nnz);
+    Operands<double> o;
+    o.arpt = a.rowptr;
+    o.acol = a.col;
+    o.aval = static_cast<const double *>(a.val);
+    o.brpt = b.rowptr;
+    o.bcol = b.col;
+    o.bval = static_cast<const double *>(b.val);
+    o.ncols = b.ncols;
+    o.brows = b.nrows;
+    h.ops[p] = o;
+    h.row_off[p] = (int)h.rows;
+    h.rows += a.nrows;
+    h.a_nnz += a.nnz;
+    h.max_rows = std::max<long long>(h.max_rows, a.nrows);
+    h.max_ncols = std::max(h.max_ncols, b.ncols);
+    h.max_brows = std::max(h.max_brows, b.nrows);
+    if (h.rows >= INT32_MAX) return NSPB_ERR_OVERFLOW;
   }
-  h.a_rows[count] = h.rows_a;
-  h.a_nnz[count] = h.nnz_a;
-  h.b_rows[count] = h.rows_b;
-  h.b_nnz[count] = h.nnz_b;
-  if (h.rows_a >= INT32_MAX || h.rows_b >= INT32_MAX || h.cols_b >= INT32_MAX ||
-      h.nnz_a > INT32_MAX || h.nnz_b > INT32_MAX)
-    return NSPB_ERR_OVERFLOW;
-  const size_t vsz = f32 ? 4 : 8;
+  h.row_off[count] = (int)h.rows;
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
   size_t off = 0;
-  h.o_da = off; off = al(off + sizeof(CatDesc) * count);
-  h.o_db = off; off = al(off + sizeof(CatDesc) * count);
-  h.o_ar = off; off = al(off + 8 * (count + 1));
-  h.o_an = off; off = al(off + 8 * (count + 1));
-  h.o_br = off; off = al(off + 8 * (count + 1));
-  h.o_bn = off; off = al(off + 8 * (count + 1));
-  h.o_sh = off; off = al(off + 4 * count);
-  h.o_arp = off; off = al(off + 4 * (h.rows_a + 1));
-  h.o_acl = off; off = al(off + 4 * h.nnz_a);
-  h.o_avl = off; off = al(off + vsz * h.nnz_a);
-  h.o_brp = off; off = al(off + 4 * (h.rows_b + 1));
-  h.o_bcl = off; off = al(off + 4 * h.nnz_b);
-  h.o_bvl = off; off = al(off + vsz * h.nnz_b);
-  h.o_crp = off; off = al(off + 4 * (h.rows_a + 1));
-  h.o_st = off; off = al(off + 4 * (count + 1));
+  h.o_ops = off; off = al(off + sizeof(Operands<double>) * count);
+  h.o_roff = off; off = al(off + 4 * (size_t)(count + 1));
+  h.o_por = off; off = al(off + 4 * (size_t)std::max<long long>(h.rows, 1));
+  h.o_crp = off; off = al(off + 4 * (size_t)(h.rows + 1));
+  h.o_st = off; off = al(off + 4 * (size_t)(count + 1));
   h.bytes = off;
   return NSPB_OK;
 }
 
-// Columns and values of every product into the block-diagonal arrays.
-static void cat_entries(const CatHost &h, char *ws, cudaStream_t s) {
-  const CatDesc *dda = reinterpret_cast<const CatDesc *>(ws + h.o_da);
-  const CatDesc *ddb = reinterpret_cast<const CatDesc *>(ws + h.o_db);
-  int *acl = reinterpret_cast<int *>(ws + h.o_acl), *bcl = reinterpret_cast<int *>(ws + h.o_bcl);
-  if (h.f32) {
-    k_cat_entries<float><<<grid2(h.max_na, h.count), 256, 0, s>>>(
-        dda, acl, reinterpret_cast<float *>(ws + h.o_avl));
-    k_cat_entries<float><<<grid2(h.max_nb, h.count), 256, 0, s>>>(
-        ddb, bcl, reinterpret_cast<float *>(ws + h.o_bvl));
-  } else {
-    k_cat_entries<double><<<grid2(h.max_na, h.count), 256, 0, s>>>(
-        dda, acl, reinterpret_cast<double *>(ws + h.o_avl));
-    k_cat_entries<double><<<grid2(h.max_nb, h.count), 256, 0, s>>>(
-        ddb, bcl, reinterpret_cast<double *>(ws + h.o_bvl));
-  }
-}
-
-// Descriptors to the device (`host` keeps the staging bytes alive until the
-// copy has run), then the row pointers and entries of the concatenation.
-static cudaError_t cat_build(const CatHost &h, char *ws, std::vector<char> &host,
-                             cudaStream_t s) {
-  host.assign(h.o_arp, 0);
-  std::memcpy(host.data() + h.o_da, h.da.data(), sizeof(CatDesc) * h.count);
-  std::memcpy(host.data() + h.o_db, h.db.data(), sizeof(CatDesc) * h.count);
-  std::memcpy(host.data() + h.o_ar, h.a_rows.data(), 8 * (h.count + 1));
-  std::memcpy(host.data() + h.o_an, h.a_nnz.data(), 8 * (h.count + 1));
-  std::memcpy(host.data() + h.o_br, h.b_rows.data(), 8 * (h.count + 1));
-  std::memcpy(host.data() + h.o_bn, h.b_nnz.data(), 8 * (h.count + 1));
-  std::memcpy(host.data() + h.o_sh, h.cshift.data(), 4 * h.count);
-  cudaError_t e = cudaMemcpyAsync(ws, host.data(), h.o_arp, cudaMemcpyHostToDevice, s);
+// Descriptors and row offsets to the device (`host` keeps the staging bytes
+// alive until the copy has run), then the row-to-product map.
+static cudaError_t table_build(const TableHost &h, char *ws, std::vector<char> &host,
+                               cudaStream_t s) {
+  host.assign(h.o_por, 0);
+  std::memcpy(host.data() + h.o_ops, h.ops.data(), sizeof(Operands<double>) * h.count);
+  std::memcpy(host.data() + h.o_roff, h.row_off.data(), 4 * (size_t)(h.count + 1));
+  cudaError_t e = cudaMemcpyAsync(ws, host.data(), h.o_por, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
-  const CatDesc *dda = reinterpret_cast<const CatDesc *>(ws + h.o_da);
-  const CatDesc *ddb = reinterpret_cast<const CatDesc *>(ws + h.o_db);
-  k_cat_rows<<<grid2(h.max_ra, h.count), 256, 0, s>>>(dda, h.rows_a, h.nnz_a,
-                                                       reinterpret_cast<int *>(ws + h.o_arp));
-  k_cat_rows<<<grid2(h.max_rb, h.count), 256, 0, s>>>(ddb, h.rows_b, h.nnz_b,
-                                                       reinterpret_cast<int *>(ws + h.o_brp));
-  cat_entries(h, ws, s);
+  if (h.rows > 0)
+    k_fill_rows<<<grid2(h.max_rows, h.count), 256, 0, s>>>(
+        reinterpret_cast<const int *>(ws + h.o_roff), reinterpret_cast<int *>(ws + h.o_por));
   return cudaGetLastError();
 }
 
-static nspb_csr_in cat_in(const CatHost &h, char *ws, bool is_a) {
-  const int32_t vt = h.f32 ? NSPB_F32 : NSPB_F64;
-  if (is_a)
-    return nspb_csr_in{(int32_t)h.rows_a, (int32_t)h.rows_b, h.nnz_a,
-                       reinterpret_cast<int *>(ws + h.o_arp), reinterpret_cast<int *>(ws + h.o_acl),
-                       ws + h.o_avl, vt, 0};
-  return nspb_csr_in{(int32_t)h.rows_b, (int32_t)h.cols_b, h.nnz_b,
-                     reinterpret_cast<int *>(ws + h.o_brp), reinterpret_cast<int *>(ws + h.o_bcl),
-                     ws + h.o_bvl, vt, 0};
+// The group as a call sees it.
+static void table_of(const TableHost &h, char *ws, Call &call) {
+  ProdTable<double> d;
+  d.ops = reinterpret_cast<const Operands<double> *>(ws + h.o_ops);
+  d.prod_of_row = reinterpret_cast<const int *>(ws + h.o_por);
+  d.row_off = reinterpret_cast<const int *>(ws + h.o_roff);
+  ProdTable<float> f;
+  f.ops = reinterpret_cast<const Operands<float> *>(ws + h.o_ops);
+  f.prod_of_row = d.prod_of_row;
+  f.row_off = d.row_off;
+  ProdInfo info;
+  info.n = (int)h.rows;
+  info.max_ncols = h.max_ncols;
+  info.nprod = h.count;
+  info.max_brows = h.max_brows;
+  call.set_table(d, f, info, h.a_nnz);
 }
 
-// Per-product row pointers into rp_all and C_cat's columns shifted back.
-static void cat_split(const CatHost &h, char *ws, long long nnz_c, int *rp_all, int *ccol,
-                      cudaStream_t s) {
-  const long long per = std::max<long long>(nnz_c / std::max(h.count, 1) * 4, 1 << 16);
-  k_split<<<grid2(per, h.count), 256, 0, s>>>(
-      reinterpret_cast<const int *>(ws + h.o_crp), reinterpret_cast<const long long *>(ws + h.o_ar),
-      reinterpret_cast<const int *>(ws + h.o_sh), rp_all, ccol);
+static void table_split(const TableHost &h, char *ws, int *rp_all, cudaStream_t s) {
+  k_split_rows<<<grid2(h.max_rows + 1, h.count), 256, 0, s>>>(
+      reinterpret_cast<const int *>(ws + h.o_crp), reinterpret_cast<const int *>(ws + h.o_roff),
+      rp_all);
 }
 
-// First C_cat entry of every product (p <= count), read back to the host.
-static cudaError_t cat_starts(const CatHost &h, char *ws, std::vector<int> &starts,
-                              cudaStream_t s) {
+// First C entry of every product (p <= count), read back to the host.
+static cudaError_t table_starts(const TableHost &h, char *ws, std::vector<int> &starts,
+                                cudaStream_t s) {
   int *d = reinterpret_cast<int *>(ws + h.o_st);
   k_gather_starts<<<grid_cap(h.count + 1), 256, 0, s>>>(
-      reinterpret_cast<const int *>(ws + h.o_crp), reinterpret_cast<const long long *>(ws + h.o_ar),
+      reinterpret_cast<const int *>(ws + h.o_crp), reinterpret_cast<const int *>(ws + h.o_roff),
       h.count, d);
   cudaError_t e = cudaGetLastError();
   starts.assign(h.count + 1, 0);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(starts.data(), d, 4 * (h.count + 1), cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(starts.data(), d, 4 * (size_t)(h.count + 1), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return e;
 }
 
-static void cat_views(const CatHost &h, const nspb_csr_in *A, const nspb_csr_in *B,
-                      const std::vector<int> &starts, int *rp_all, int *ccol, double *cval,
-                      nspb_csr_out *C) {
+static void table_views(const TableHost &h, const nspb_csr_in *A, const nspb_csr_in *B,
+                        const std::vector<int> &starts, int *rp_all, int *ccol, double *cval,
+                        nspb_csr_out *C) {
   for (int p = 0; p < h.count; ++p) {
     C[p].nrows = A[p].nrows;
     C[p].ncols = B[p].ncols;
     C[p].nnz = starts[p + 1] - starts[p];
-    C[p].rowptr = rp_all + h.a_rows[p] + p;
+    C[p].rowptr = rp_all + h.row_off[p] + p;
     C[p].col = ccol + starts[p];
     C[p].val = cval + starts[p];
     C[p].capacity = C[p].nnz;
   }
 }
 
-// One group of products as one block-diagonal product. On success C[p] are
-// views into two allocations (C_cat col/val) plus the row-pointer block; the
-// three base pointers are appended to owners.
+// One group of products through one pipeline. On success C[p] are views into
+// two allocations (C col/val) plus the row-pointer block; the three base
+// pointers are appended to owners.
 static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
                          const nspb_opts &o, nspb_stats *stats, void **owners, int *n_owners) {
   cudaStream_t s = static_cast<cudaStream_t>(o.stream);
-  CatHost h;
-  int st = cat_layout(count, A, B, fp32_inputs(o.precision), h);
+  TableHost h;
+  int st = table_layout(count, A, B, fp32_inputs(o.precision), h);
   if (st) return st;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return NSPB_ERR_NO_DEVICE;
-  }
+  Call call;
+  if ((st = call.init(&A[0], &B[0], &o))) return st;
   char *ws = nullptr;
   if ((st = scratch_alloc(reinterpret_cast<void **>(&ws), h.bytes, s))) return st;
   std::vector<char> host;
-  cudaError_t e = cat_build(h, ws, host, s);
+  cudaError_t e = table_build(h, ws, host, s);
   if (e != cudaSuccess) {
     g_last_cuda = (int)e;
     cudaGetLastError();
@@ -298,41 +218,40 @@ static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, 
     scratch_free(ws, s);
     return NSPB_ERR_CUDA;
   }
-  // the product of the block-diagonal operands, C_cat arrays allocated here
-  const nspb_csr_in Acat = cat_in(h, ws, true), Bcat = cat_in(h, ws, false);
-  nspb_csr_out Ccat;
-  std::memset(&Ccat, 0, sizeof(Ccat));
-  Ccat.rowptr = reinterpret_cast<int *>(ws + h.o_crp);
-  st = nspb_spgemm(&Acat, &Bcat, &Ccat, &o, stats);
-  if (st) {
-    cudaStreamSynchronize(s);
-    scratch_free(ws, s);
-    return st;
-  }
-  int *rp_all = nullptr;
-  st = alloc_out(reinterpret_cast<void **>(&rp_all), 4 * (size_t)(h.rows_a + count));
+  table_of(h, ws, call);
+  int *crp = reinterpret_cast<int *>(ws + h.o_crp);
+  int64_t nnz = 0;
+  int *ccol = nullptr, *rp_all = nullptr;
+  double *cval = nullptr;
+  st = call.symbolic(crp, &nnz);
+  if (!st) st = alloc_out(reinterpret_cast<void **>(&ccol), (size_t)nnz * 4);
+  if (!st) st = alloc_out(reinterpret_cast<void **>(&cval), (size_t)nnz * 8);
+  if (!st) st = call.numeric(crp, ccol, cval);
+  if (!st) st = call.finish(stats);
+  if (!st) st = alloc_out(reinterpret_cast<void **>(&rp_all), 4 * (size_t)(h.rows + count));
   std::vector<int> starts;
   if (!st) {
-    cat_split(h, ws, Ccat.nnz, rp_all, Ccat.col, s);
+    table_split(h, ws, rp_all, s);
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cat_starts(h, ws, starts, s);
+    if (e == cudaSuccess) e = table_starts(h, ws, starts, s);
     if (e != cudaSuccess) {
       g_last_cuda = (int)e;
+      cudaGetLastError();
       st = NSPB_ERR_CUDA;
     }
   }
+  cudaStreamSynchronize(s);
   scratch_free(ws, s);
   if (st) {
-    cudaStreamSynchronize(s);
     if (rp_all) cudaFree(rp_all);
-    cudaFree(Ccat.col);
-    cudaFree(Ccat.val);
+    if (ccol) cudaFree(ccol);
+    if (cval) cudaFree(cval);
     return st;
   }
-  cat_views(h, A, B, starts, rp_all, Ccat.col, Ccat.val, C);
+  table_views(h, A, B, starts, rp_all, ccol, cval, C);
   owners[(*n_owners)++] = rp_all;
-  owners[(*n_owners)++] = Ccat.col;
-  owners[(*n_owners)++] = Ccat.val;
+  owners[(*n_owners)++] = ccol;
+  owners[(*n_owners)++] = cval;
   return NSPB_OK;
 }
 
@@ -408,20 +327,20 @@ extern "C" int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_c
 // ---- plans: the numeric phase of a fixed structure replayed from a CUDA graph --
 namespace nspb {
 
-// One group of a plan: one product, or several as one block-diagonal product.
+// One group of a plan: one product, or several through a product table.
 struct PlanGroup {
-  bool cat = false;            // block-diagonal operands
-  CatHost h;                   // their layout (cat)
-  Call call;                   // the product whose numeric phase is captured
-  char *ws_cat = nullptr;      // concatenated operands and C_cat's row pointer
+  bool multi = false;          // several products (a table)
+  TableHost h;                 // the table's layout (multi)
+  Call call;                   // the products whose numeric phase is captured
+  char *ws_tab = nullptr;      // the table and the group's row pointer (multi)
   char *ws_call = nullptr;     // the call's scratch (bins, permutation, counters)
   int *crp = nullptr;          // C's row pointer of a single product
-  int *rp_all = nullptr;       // per-product row pointers (cat)
+  int *rp_all = nullptr;       // per-product row pointers (multi)
   int *ccol = nullptr;
   double *cval = nullptr;
   long long nnz = 0;
   ~PlanGroup() {
-    for (void *p : {(void *)ws_cat, (void *)ws_call, (void *)crp, (void *)rp_all, (void *)ccol,
+    for (void *p : {(void *)ws_tab, (void *)ws_call, (void *)crp, (void *)rp_all, (void *)ccol,
                     (void *)cval})
       if (p) cudaFree(p);
   }
@@ -465,24 +384,15 @@ int dev_alloc(T **p, size_t count) {
 }
 
 // The numeric phase of a group as launched on every execution: counters
-// zeroed, operand entries concatenated, bin kernels, split.
+// zeroed, then the bin kernels, which read the operands' current values
+// where they lie (structure and C's row pointers do not change).
 int group_numeric(PlanGroup &G, cudaStream_t s) {
   G.call.s = s;
   if (G.call.n == 0) return NSPB_OK;  // no rows: no scratch, nothing to compute
   cudaError_t e = cudaMemsetAsync(G.call.ctr, 0, sizeof(DevCounters), s);
   if (e != cudaSuccess) return plan_fail(e);
-  if (G.cat) {
-    cat_entries(G.h, G.ws_cat, s);
-    if ((e = cudaGetLastError()) != cudaSuccess) return plan_fail(e);
-  }
-  const int *crp = G.cat ? reinterpret_cast<int *>(G.ws_cat + G.h.o_crp) : G.crp;
-  int st = G.call.numeric(crp, G.ccol, G.cval);
-  if (st) return st;
-  if (G.cat) {
-    cat_split(G.h, G.ws_cat, G.nnz, G.rp_all, G.ccol, s);
-    if ((e = cudaGetLastError()) != cudaSuccess) return plan_fail(e);
-  }
-  return NSPB_OK;
+  const int *crp = G.multi ? reinterpret_cast<int *>(G.ws_tab + G.h.o_crp) : G.crp;
+  return G.call.numeric(crp, G.ccol, G.cval);
 }
 
 void add_stats(nspb_stats &t, const nspb_stats &g) {
@@ -504,35 +414,39 @@ int group_create(int count, const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr
                  const nspb_opts &o, nspb_stats *stats, std::unique_ptr<PlanGroup> &out) {
   cudaStream_t s = static_cast<cudaStream_t>(o.stream);
   std::unique_ptr<PlanGroup> G(new PlanGroup);
-  G->cat = count > 1;
+  G->multi = count > 1;
   int st;
-  nspb_csr_in a = A[0], b = B[0];
-  if (G->cat) {
-    if ((st = cat_layout(count, A, B, fp32_inputs(o.precision), G->h))) return st;
-    if ((st = dev_alloc(&G->ws_cat, G->h.bytes))) return st;
+  if ((st = G->call.init(&A[0], &B[0], &o))) return st;
+  if (G->multi) {
+    if ((st = table_layout(count, A, B, fp32_inputs(o.precision), G->h))) return st;
+    if ((st = dev_alloc(&G->ws_tab, G->h.bytes))) return st;
     std::vector<char> host;
-    cudaError_t e = cat_build(G->h, G->ws_cat, host, s);
+    cudaError_t e = table_build(G->h, G->ws_tab, host, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // `host` is released below
     if (e != cudaSuccess) return plan_fail(e);
-    a = cat_in(G->h, G->ws_cat, true);
-    b = cat_in(G->h, G->ws_cat, false);
+    table_of(G->h, G->ws_tab, G->call);
   }
-  if ((st = G->call.init(&a, &b, &o))) return st;
   const size_t wb = G->call.scratch_bytes();
   if ((st = dev_alloc(&G->ws_call, wb))) return st;
   G->call.ext_ws = G->ws_call;
   G->call.ext_bytes = wb;
   int *crp = nullptr;
-  if (G->cat) {
-    crp = reinterpret_cast<int *>(G->ws_cat + G->h.o_crp);
+  if (G->multi) {
+    crp = reinterpret_cast<int *>(G->ws_tab + G->h.o_crp);
   } else {
-    if ((st = dev_alloc(&G->crp, (size_t)a.nrows + 1))) return st;
+    if ((st = dev_alloc(&G->crp, (size_t)A[0].nrows + 1))) return st;
     crp = G->crp;
   }
   int64_t nnz = 0;
   if ((st = G->call.symbolic(crp, &nnz))) return st;
   G->nnz = nnz;
   if ((st = dev_alloc(&G->ccol, (size_t)nnz)) || (st = dev_alloc(&G->cval, (size_t)nnz))) return st;
-  if (G->cat && (st = dev_alloc(&G->rp_all, (size_t)(G->h.rows_a + count)))) return st;
+  if (G->multi) {
+    if ((st = dev_alloc(&G->rp_all, (size_t)(G->h.rows + count)))) return st;
+    table_split(G->h, G->ws_tab, G->rp_all, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return plan_fail(e);
+  }
   // one pass on the caller's stream (fills C and the launch caches), checked;
   // the pass zeroes the device counters, so the symbolic counts are kept
   const DevCounters sym = G->call.h;
@@ -555,11 +469,11 @@ int group_create(int count, const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr
     gs.max_row_err = comp_bound(hc.max_comp_deg);
   }
   if (stats) add_stats(*stats, gs);
-  if (G->cat) {
+  if (G->multi) {
     std::vector<int> starts;
-    cudaError_t e = cat_starts(G->h, G->ws_cat, starts, s);
+    cudaError_t e = table_starts(G->h, G->ws_tab, starts, s);
     if (e != cudaSuccess) return plan_fail(e);
-    cat_views(G->h, A, B, starts, G->rp_all, G->ccol, G->cval, C);
+    table_views(G->h, A, B, starts, G->rp_all, G->ccol, G->cval, C);
   } else {
     C[0].nrows = A[0].nrows;
     C[0].ncols = B[0].ncols;

@@ -9,9 +9,25 @@
 
 #include <type_traits>
 
+#include "internal.h"
+
 namespace cg = cooperative_groups;
 
 namespace nspb {
+
+// ---- operands of a row ---------------------------------------------------------
+// The operands of global row r of a call and the row's index inside its
+// product (see ProdTable in internal.h).
+template <typename VT>
+__device__ __forceinline__ int prod_row(const ProdTable<VT> &t, int r, Operands<VT> &o) {
+  if (!t.prod_of_row) {
+    o = t.one;
+    return r;
+  }
+  const int p = __ldg(t.prod_of_row + r);
+  o = t.ops[p];
+  return r - __ldg(t.row_off + p);
+}
 
 // ---- error word bits (device -> host) ---------------------------------------
 // A kernel never traps or spins forever: a bounded loop that runs out sets a

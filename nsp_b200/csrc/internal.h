@@ -27,6 +27,61 @@ struct CsrDev {
   const float *val32 = nullptr;  // fp32 operands (FP32_COMP mode)
 };
 
+// One product's operands as the row kernels read them (device pointers).
+// Layout-identical for every VT, so a table can be viewed as Operands<void>
+// by the kernels that read no values.
+template <typename VT>
+struct Operands {
+  const int *arpt = nullptr;
+  const int *acol = nullptr;
+  const VT *aval = nullptr;
+  const int *brpt = nullptr;
+  const int *bcol = nullptr;
+  const VT *bval = nullptr;
+  int ncols = 0;  // columns of B
+  int brows = 0;  // rows of B
+};
+
+// The products a call computes, as the row kernels see them. A call's rows
+// are numbered globally; one product (prod_of_row null) is `one`, held by
+// value in the kernel parameters. A batch of products keeps a device array of
+// Operands, the product of every global A row and each product's first global
+// row: kernels read A and B where they lie, and nothing is concatenated.
+template <typename VT>
+struct ProdTable {
+  Operands<VT> one;
+  const Operands<VT> *ops = nullptr;
+  const int *prod_of_row = nullptr;
+  const int *row_off = nullptr;
+};
+
+template <typename VT>
+inline ProdTable<void> structure_of(const ProdTable<VT> &t) {
+  ProdTable<void> s;
+  s.one.arpt = t.one.arpt;
+  s.one.acol = t.one.acol;
+  s.one.aval = t.one.aval;
+  s.one.brpt = t.one.brpt;
+  s.one.bcol = t.one.bcol;
+  s.one.bval = t.one.bval;
+  s.one.ncols = t.one.ncols;
+  s.one.brows = t.one.brows;
+  s.ops = reinterpret_cast<const Operands<void> *>(t.ops);
+  s.prod_of_row = t.prod_of_row;
+  s.row_off = t.row_off;
+  return s;
+}
+
+// What the host launchers need besides the table: the call's rows, the
+// largest B column count (bitmap windows of the long-row kernels) and the
+// number of products.
+struct ProdInfo {
+  int n = 0;
+  int max_ncols = 0;
+  int nprod = 1;
+  int max_brows = 0;
+};
+
 // Flag bits written by launch_check_sorted.
 enum : int { B_UNSORTED = 1 };
 
@@ -45,6 +100,9 @@ struct CompArgs {
 
 // ---- rowinfo.cu -----------------------------------------------------------------
 cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s);
+// The B rows of every product of a table (ops: device array of nprod entries).
+cudaError_t launch_check_sorted_table(const Operands<void> *ops, int nprod, int max_brows,
+                                      int *flags, cudaStream_t s);
 // row_nz[i] = min(intprod_i, ncols(B)); sym_counts[b] += rows of symbolic bin b
 // (rows with zero products are not binned); *total_ip += sum of intprod_i.
 // row_ip (optional) receives intprod_i as int64.
@@ -52,7 +110,7 @@ cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s);
 // would, from the rows read here. long_list / long_count (may be NULL; n ints and
 // a zeroed counter): rows of more than 1024 A entries are listed there and
 // counted by a second kernel, a block per row.
-cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
+cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *row_nz,
                            int64_t *row_ip, int *sym_counts,
                            unsigned long long *total_ip, int *flags, int *long_list,
                            int *long_count, cudaStream_t s);
@@ -89,8 +147,8 @@ cudaError_t launch_num_hist(const int *crpt, int n, int *num_counts,
 // ticket: a zeroed counter for this launch (block-per-row kernels hand out
 // rows with it). b_sorted: B rows strictly increasing (a row's column span
 // then comes from the ends of the B rows it touches).
-cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const CsrDev &A,
-                                const CsrDev &B, const int *rows, int count,
+cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTable<void> &t,
+                                const ProdInfo &info, const int *rows, int count,
                                 int *row_nz, int *err, int *ticket, cudaStream_t s);
 
 // ---- numeric.cu -----------------------------------------------------------------
@@ -99,7 +157,7 @@ cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const CsrDev 
 // b_sorted: B rows strictly increasing (long rows take their column span
 // from the ends of the B rows they touch).
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
-                               const CsrDev &A, const CsrDev &B,
+                               const ProdTable<double> &t, const ProdInfo &info,
                                const int *crpt, int *ccol, double *cval,
                                const int *rows, int count, int *err, int *ticket,
                                int tshift, cudaStream_t s);
@@ -110,9 +168,9 @@ cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
 // counts the fp64 rows, *max_deg receives the largest A-row degree among the
 // pair rows.
 cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorted,
-                                    const CsrDev &A, const CsrDev &B, const int *crpt,
-                                    int *ccol, double *cval, const int *rows, int count,
-                                    int nmax, int *redo, int *max_deg, int *err,
+                                    const ProdTable<float> &t, const ProdInfo &info,
+                                    const int *crpt, int *ccol, double *cval, const int *rows,
+                                    int count, int nmax, int *redo, int *max_deg, int *err,
                                     int *ticket, int tshift, cudaStream_t s);
 
 // ---- rowgroup.cu ----------------------------------------------------------------
@@ -121,13 +179,13 @@ cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorte
 // increasing. tshift 0 gives tables of four times the bin's row limit, -1
 // twice. depth: B rows whose loads are issued together before their inserts
 // (1, 2 or 4).
-cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
-                              const CsrDev &B,
-                              const int *crpt, int *ccol, double *cval, const int *rows,
-                              int count, int *err, cudaStream_t s);
-cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
-                                   const CsrDev &B, const int *crpt, int *ccol, double *cval,
-                                   const int *rows, int count, int nmax, int *redo, int *max_deg,
-                                   int *err, cudaStream_t s);
+cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth,
+                              const ProdTable<double> &t, const int *crpt, int *ccol,
+                              double *cval, const int *rows, int count, int *err,
+                              cudaStream_t s);
+cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth,
+                                   const ProdTable<float> &t, const int *crpt, int *ccol,
+                                   double *cval, const int *rows, int count, int nmax,
+                                   int *redo, int *max_deg, int *err, cudaStream_t s);
 
 }  // namespace nspb

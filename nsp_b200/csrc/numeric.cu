@@ -66,10 +66,7 @@ struct NumGroupCfg {
 // COMP: fp32 inputs with the error-free pair accumulation for short rows.
 template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>
 __global__ void __launch_bounds__(256)
-    k_num_group(const int *__restrict__ arpt, const int *__restrict__ acol,
-                const VT *__restrict__ aval, const int *__restrict__ brpt,
-                const int *__restrict__ bcol, const VT *__restrict__ bval,
-                const int *__restrict__ crpt, int *__restrict__ ccol,
+    k_num_group(const ProdTable<VT> src, const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
                 int *__restrict__ err, CompArgs comp) {
   using C = NumGroupCfg<G, LOG2T>;
@@ -94,7 +91,11 @@ __global__ void __launch_bounds__(256)
     for (int s = lane; s < C::T / 4; s += G)
       reinterpret_cast<int4 *>(keys)[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
     tile.sync();
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<VT> op;
+    const int lr = prod_row(src, row, op);
+    const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
+    const VT *aval = op.aval, *bval = op.bval;
+    const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     // compensated mode: pair accumulation when the row's Dot2 bound allows it
     const bool pair = COMP && OWNED && (a1 - a0) <= comp.nmax;
     float2 *vals2 = reinterpret_cast<float2 *>(vals);
@@ -281,10 +282,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *red, int *tot) {
 
 template <int LOG2T, typename VT>
 __global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
-    k_num_block(const int *__restrict__ arpt, const int *__restrict__ acol,
-                const VT *__restrict__ aval, const int *__restrict__ brpt,
-                const int *__restrict__ bcol, const VT *__restrict__ bval,
-                const int *__restrict__ crpt, int *__restrict__ ccol,
+    k_num_block(const ProdTable<VT> src, const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
                 int *__restrict__ err, int *__restrict__ redo, int *__restrict__ ticket) {
   constexpr int T = 1 << LOG2T, H = T / 2, NB = T / 2;
@@ -315,9 +313,11 @@ __global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
       s_mx = -1;
     }
     __syncthreads();
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<VT> op;
+    const int lr = prod_row(src, row, op);
+    const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     int mn = 0x7fffffff, mx = -1;
-    row_products<kNumBlockThreads>(acol, aval, brpt, bcol, bval, a0, a1, rq,
+    row_products<kNumBlockThreads>(op.acol, op.aval, op.brpt, op.bcol, op.bval, a0, a1, rq,
                                    [&](int key, double a, double b) {
       num_insert<LOG2T, false, true>(keys, vals, key, __dmul_rn(a, b), err);
       mn = min(mn, key);
@@ -453,10 +453,7 @@ __device__ __forceinline__ void red_add_global_keep(double *p, double v, unsigne
 
 template <typename VT, int MINB>
 __global__ void __launch_bounds__(kRankThreads, MINB)
-    k_num_rank(const int *__restrict__ arpt, const int *__restrict__ acol,
-               const VT *__restrict__ aval, const int *__restrict__ brpt,
-               const int *__restrict__ bcol, const VT *__restrict__ bval, int ncols,
-               int b_sorted, int pl_max, const int *__restrict__ crpt,
+    k_num_rank(const ProdTable<VT> src, int b_sorted, int pl_max, const int *__restrict__ crpt,
                int *__restrict__ ccol, double *__restrict__ cval,
                const int *__restrict__ rows, int count, int *__restrict__ err,
                int *__restrict__ redo, int *__restrict__ ticket) {
@@ -475,7 +472,12 @@ __global__ void __launch_bounds__(kRankThreads, MINB)
   for (int q = threadIdx.x; q < max_words; q += kRankThreads) bm64[q] = 0ull;
   for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<VT> op;
+    const int lr = prod_row(src, row, op);
+    const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
+    const VT *aval = op.aval, *bval = op.bval;
+    const int ncols = op.ncols;
+    const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     const int row_end = crpt[row + 1];
     int off = crpt[row];
     bool bad = false;  // block-uniform
@@ -588,42 +590,39 @@ __global__ void __launch_bounds__(kRankThreads, MINB)
 }
 
 template <typename VT>
-static cudaError_t run_num_rank(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
-                                bool b_sorted, const int *crpt, int *ccol, double *cval,
-                                const int *rows, int count, int *err, int *redo, int *ticket,
-                                cudaStream_t s) {
-  const int pl = rank_per_log2((int)std::min<long long>(B.ncols, kRankMaxCols));
+static cudaError_t run_num_rank(const ProdTable<VT> &t, const ProdInfo &info, bool b_sorted,
+                                const int *crpt, int *ccol, double *cval, const int *rows,
+                                int count, int *err, int *redo, int *ticket, cudaStream_t s) {
+  const int pl = rank_per_log2((int)std::min<long long>(info.max_ncols, kRankMaxCols));
   const int smem = rank_smem(pl);
   auto kern = rank_minb(pl) == 1 ? k_num_rank<VT, 1> : k_num_rank<VT, 2>;
   const int grid = persistent_grid((const void *)kern, kRankThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  kern<<<grid, kRankThreads, smem, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, B.ncols,
-                                        b_sorted ? 1 : 0, pl, crpt, ccol, cval, rows, count, err,
-                                        redo, ticket);
+  kern<<<grid, kRankThreads, smem, s>>>(t, b_sorted ? 1 : 0, pl, crpt, ccol, cval, rows, count,
+                                        err, redo, ticket);
   return cudaGetLastError();
 }
 
 // ---- dispatch ------------------------------------------------------------------------
 template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>
-static cudaError_t run_num_group(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
-                                 const int *crpt, int *ccol, double *cval, const int *rows,
-                                 int count, int *err, CompArgs comp, cudaStream_t s) {
+static cudaError_t run_num_group(const ProdTable<VT> &t, const int *crpt, int *ccol,
+                                 double *cval, const int *rows, int count, int *err,
+                                 CompArgs comp, cudaStream_t s) {
   using C = NumGroupCfg<G, LOG2T>;
   const void *f = (const void *)k_num_group<G, LOG2T, OWNED, VT, COMP>;
   const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   k_num_group<G, LOG2T, OWNED, VT, COMP><<<grid, C::THREADS, C::SMEM, s>>>(
-      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, comp);
+      t, crpt, ccol, cval, rows, count, err, comp);
   return cudaGetLastError();
 }
 
 template <int G, bool OWNED, typename VT, bool COMP>
-static cudaError_t num_group_bin(int bin, const CsrDev &A, const CsrDev &B, const VT *av,
-                                 const VT *bv, const int *crpt, int *ccol, double *cval,
-                                 const int *rows, int count, int *err, CompArgs comp,
-                                 int tshift, cudaStream_t s) {
+static cudaError_t num_group_bin(int bin, const ProdTable<VT> &t, const int *crpt, int *ccol,
+                                 double *cval, const int *rows, int count, int *err,
+                                 CompArgs comp, int tshift, cudaStream_t s) {
 #define NSPB_NG(L2T) \
-  run_num_group<G, L2T, OWNED, VT, COMP>(A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, s)
+  run_num_group<G, L2T, OWNED, VT, COMP>(t, crpt, ccol, cval, rows, count, err, comp, s)
   // bin b holds rows of at most 16 << b entries; its table has 32 << (b + tshift)
   // slots (load <= 1/2 or 1/4), 1024 at most
   switch (std::min(5 + bin + tshift, 10)) {
@@ -638,28 +637,27 @@ static cudaError_t num_group_bin(int bin, const CsrDev &A, const CsrDev &B, cons
 }
 
 template <int LOG2T, typename VT>
-static cudaError_t run_num_block(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
-                                 const int *crpt, int *ccol, double *cval, const int *rows,
-                                 int count, int *err, int *redo, int *ticket, cudaStream_t s) {
+static cudaError_t run_num_block(const ProdTable<VT> &t, const int *crpt, int *ccol,
+                                 double *cval, const int *rows, int count, int *err, int *redo,
+                                 int *ticket, cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
   const int smem = T * 12 + (T / 2) * 12 + (T / 2) * 4;
   const void *f = (const void *)k_num_block<LOG2T, VT>;
   const int grid = persistent_grid(f, kNumBlockThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_block<LOG2T, VT><<<grid, kNumBlockThreads, smem, s>>>(
-      A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval, rows, count, err, redo, ticket);
+  k_num_block<LOG2T, VT><<<grid, kNumBlockThreads, smem, s>>>(t, crpt, ccol, cval, rows, count,
+                                                               err, redo, ticket);
   return cudaGetLastError();
 }
 
 template <typename VT, bool COMP>
-static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, const CsrDev &A,
-                                 const CsrDev &B, const VT *av, const VT *bv, const int *crpt,
+static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted,
+                                 const ProdTable<VT> &t, const ProdInfo &info, const int *crpt,
                                  int *ccol, double *cval, const int *rows, int count, int *err,
                                  CompArgs comp, int *ticket, int tshift, cudaStream_t s) {
   if (bin < kNumGroupBins) {
 #define NSPB_GB(GL, OW) \
-  num_group_bin<GL, OW, VT, COMP>(bin, A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, \
-                                  tshift, s)
+  num_group_bin<GL, OW, VT, COMP>(bin, t, crpt, ccol, cval, rows, count, err, comp, tshift, s)
     if (owned) {
       if (lanes == 8) return NSPB_GB(8, true);
       if (lanes == 16) return NSPB_GB(16, true);
@@ -672,40 +670,37 @@ static cudaError_t numeric_bin_t(int bin, int lanes, bool owned, bool b_sorted, 
   }
   int *redo = COMP ? comp.redo : nullptr;
   if (bin >= kRankFromBin)
-    return run_num_rank<VT>(A, B, av, bv, b_sorted, crpt, ccol, cval, rows, count, err, redo,
+    return run_num_rank<VT>(t, info, b_sorted, crpt, ccol, cval, rows, count, err, redo,
                             ticket, s);
   switch (bin) {
     case kNumGroupBins:
-      return run_num_block<11, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo,
-                                  ticket, s);
+      return run_num_block<11, VT>(t, crpt, ccol, cval, rows, count, err, redo, ticket, s);
     case kNumGroupBins + 1:
-      return run_num_block<12, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo,
-                                  ticket, s);
+      return run_num_block<12, VT>(t, crpt, ccol, cval, rows, count, err, redo, ticket, s);
     default:
-      return run_num_block<13, VT>(A, B, av, bv, crpt, ccol, cval, rows, count, err, redo,
-                                  ticket, s);
+      return run_num_block<13, VT>(t, crpt, ccol, cval, rows, count, err, redo, ticket, s);
   }
 }
 
 cudaError_t launch_numeric_bin(int bin, int lanes, bool owned, bool b_sorted,
-                               const CsrDev &A, const CsrDev &B, const int *crpt,
-                               int *ccol, double *cval, const int *rows, int count,
-                               int *err, int *ticket, int tshift, cudaStream_t s) {
+                               const ProdTable<double> &t, const ProdInfo &info,
+                               const int *crpt, int *ccol, double *cval, const int *rows,
+                               int count, int *err, int *ticket, int tshift, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  return numeric_bin_t<double, false>(bin, lanes, owned, b_sorted, A, B, A.val, B.val, crpt,
-                                      ccol, cval, rows, count, err, CompArgs{0, nullptr, nullptr},
-                                      ticket, tshift, s);
+  return numeric_bin_t<double, false>(bin, lanes, owned, b_sorted, t, info, crpt, ccol, cval,
+                                      rows, count, err, CompArgs{0, nullptr, nullptr}, ticket,
+                                      tshift, s);
 }
 
 cudaError_t launch_numeric_comp_bin(int bin, int lanes, bool owned, bool b_sorted,
-                                    const CsrDev &A, const CsrDev &B, const int *crpt,
-                                    int *ccol, double *cval, const int *rows, int count,
-                                    int nmax, int *redo, int *max_deg, int *err,
+                                    const ProdTable<float> &t, const ProdInfo &info,
+                                    const int *crpt, int *ccol, double *cval, const int *rows,
+                                    int count, int nmax, int *redo, int *max_deg, int *err,
                                     int *ticket, int tshift, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
-  return numeric_bin_t<float, true>(bin, lanes, owned, b_sorted, A, B, A.val32, B.val32, crpt,
-                                    ccol, cval, rows, count, err, CompArgs{nmax, redo, max_deg},
-                                    ticket, tshift, s);
+  return numeric_bin_t<float, true>(bin, lanes, owned, b_sorted, t, info, crpt, ccol, cval, rows,
+                                    count, err, CompArgs{nmax, redo, max_deg}, ticket, tshift,
+                                    s);
 }
 
 }  // namespace nspb

@@ -96,10 +96,8 @@ struct NumRgCfg {
 
 template <int G, int LOG2H, int LOG2T, typename VT, bool COMP, int D>
 __global__ void __launch_bounds__(256)
-    k_num_rg(const int *__restrict__ arpt, const int *__restrict__ acol,
-             const VT *__restrict__ aval, const int *__restrict__ brpt,
-             const int *__restrict__ bcol, const VT *__restrict__ bval,
-             const int *__restrict__ crpt, int *__restrict__ ccol, double *__restrict__ cval,
+    k_num_rg(const ProdTable<VT> src, const int *__restrict__ crpt, int *__restrict__ ccol,
+             double *__restrict__ cval,
              const int *__restrict__ rows, int count, int *__restrict__ err, CompArgs comp) {
   using C = NumRgCfg<G, LOG2H, LOG2T>;
   constexpr int T = C::T, H = C::H, V = C::V;
@@ -128,7 +126,11 @@ __global__ void __launch_bounds__(256)
   int my_max_deg = 0, my_redo = 0;  // compensated mode, flushed once per group
   for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
     const int row = rows ? rows[r] : r;
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<VT> op;
+    const int lr = prod_row(src, row, op);
+    const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
+    const VT *aval = op.aval, *bval = op.bval;
+    const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     const bool pair = COMP && (a1 - a0) <= comp.nmax;
     int mn = 0x7fffffff, mx = -1;
     // -- walk: one B row per step, keys of a step distinct (B rows strictly
@@ -311,30 +313,27 @@ __global__ void __launch_bounds__(256)
 }
 
 template <int G, int LOG2H, int LOG2T, typename VT, bool COMP>
-static cudaError_t run_num_rg(const CsrDev &A, const CsrDev &B, const VT *av, const VT *bv,
-                              const int *crpt, int *ccol, double *cval, const int *rows,
-                              int count, int *err, CompArgs comp, int depth, cudaStream_t s) {
+static cudaError_t run_num_rg(const ProdTable<VT> &t, const int *crpt, int *ccol, double *cval,
+                              const int *rows, int count, int *err, CompArgs comp, int depth,
+                              cudaStream_t s) {
   using C = NumRgCfg<G, LOG2H, LOG2T>;
   auto kern = depth >= 4 ? k_num_rg<G, LOG2H, LOG2T, VT, COMP, 4>
             : depth >= 2 ? k_num_rg<G, LOG2H, LOG2T, VT, COMP, 2>
                          : k_num_rg<G, LOG2H, LOG2T, VT, COMP, 1>;
   const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  kern<<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, av, B.rpt, B.col, bv, crpt, ccol, cval,
-                                         rows, count, err, comp);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, crpt, ccol, cval, rows, count, err, comp);
   return cudaGetLastError();
 }
 
 // Numeric bin b holds rows of at most 16 << b entries (H); the table has
 // 4H slots (load <= 1/4) or, with tshift = -1, 2H.
 template <int G, typename VT, bool COMP>
-static cudaError_t num_rg_bin(int bin, int tshift, int depth, const CsrDev &A, const CsrDev &B,
-                              const VT *av, const VT *bv, const int *crpt, int *ccol,
-                              double *cval, const int *rows, int count, int *err,
-                              CompArgs comp, cudaStream_t s) {
+static cudaError_t num_rg_bin(int bin, int tshift, int depth, const ProdTable<VT> &t,
+                              const int *crpt, int *ccol, double *cval, const int *rows,
+                              int count, int *err, CompArgs comp, cudaStream_t s) {
 #define NSPB_NRG(L2H, L2T) \
-  run_num_rg<G, L2H, L2T, VT, COMP>(A, B, av, bv, crpt, ccol, cval, rows, count, err, comp, \
-                                    depth, s)
+  run_num_rg<G, L2H, L2T, VT, COMP>(t, crpt, ccol, cval, rows, count, err, comp, depth, s)
   const bool big = tshift >= 0;
   switch (bin) {
     case 0: return big ? NSPB_NRG(4, 6) : NSPB_NRG(4, 5);
@@ -347,36 +346,36 @@ static cudaError_t num_rg_bin(int bin, int tshift, int depth, const CsrDev &A, c
 #undef NSPB_NRG
 }
 
-cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
-                              const CsrDev &B,
-                              const int *crpt, int *ccol, double *cval, const int *rows,
-                              int count, int *err, cudaStream_t s) {
+cudaError_t launch_numeric_rg(int bin, int lanes, int tshift, int depth,
+                              const ProdTable<double> &t, const int *crpt, int *ccol,
+                              double *cval, const int *rows, int count, int *err,
+                              cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   const CompArgs none{0, nullptr, nullptr};
   if (lanes == 8)
-    return num_rg_bin<8, double, false>(bin, tshift, depth, A, B, A.val, B.val, crpt, ccol, cval, rows,
-                                        count, err, none, s);
+    return num_rg_bin<8, double, false>(bin, tshift, depth, t, crpt, ccol, cval, rows, count,
+                                        err, none, s);
   if (lanes == 16)
-    return num_rg_bin<16, double, false>(bin, tshift, depth, A, B, A.val, B.val, crpt, ccol, cval, rows,
-                                         count, err, none, s);
-  return num_rg_bin<32, double, false>(bin, tshift, depth, A, B, A.val, B.val, crpt, ccol, cval, rows,
-                                       count, err, none, s);
+    return num_rg_bin<16, double, false>(bin, tshift, depth, t, crpt, ccol, cval, rows, count,
+                                         err, none, s);
+  return num_rg_bin<32, double, false>(bin, tshift, depth, t, crpt, ccol, cval, rows, count, err,
+                                       none, s);
 }
 
-cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth, const CsrDev &A,
-                                   const CsrDev &B, const int *crpt, int *ccol, double *cval,
-                                   const int *rows, int count, int nmax, int *redo, int *max_deg,
-                                   int *err, cudaStream_t s) {
+cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth,
+                                   const ProdTable<float> &t, const int *crpt, int *ccol,
+                                   double *cval, const int *rows, int count, int nmax,
+                                   int *redo, int *max_deg, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   const CompArgs comp{nmax, redo, max_deg};
   if (lanes == 8)
-    return num_rg_bin<8, float, true>(bin, tshift, depth, A, B, A.val32, B.val32, crpt, ccol, cval, rows,
-                                      count, err, comp, s);
+    return num_rg_bin<8, float, true>(bin, tshift, depth, t, crpt, ccol, cval, rows, count, err,
+                                      comp, s);
   if (lanes == 16)
-    return num_rg_bin<16, float, true>(bin, tshift, depth, A, B, A.val32, B.val32, crpt, ccol, cval,
-                                       rows, count, err, comp, s);
-  return num_rg_bin<32, float, true>(bin, tshift, depth, A, B, A.val32, B.val32, crpt, ccol, cval, rows,
-                                     count, err, comp, s);
+    return num_rg_bin<16, float, true>(bin, tshift, depth, t, crpt, ccol, cval, rows, count, err,
+                                       comp, s);
+  return num_rg_bin<32, float, true>(bin, tshift, depth, t, crpt, ccol, cval, rows, count, err,
+                                     comp, s);
 }
 
 }  // namespace nspb

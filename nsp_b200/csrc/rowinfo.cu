@@ -39,6 +39,30 @@ cudaError_t launch_check_sorted(const CsrDev &B, int *flags, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Every product's B: blockIdx.y is the product, blocks stride over its rows.
+__global__ void __launch_bounds__(256)
+    k_check_sorted_table(const Operands<void> *__restrict__ ops, int *__restrict__ flags) {
+  const Operands<void> o = ops[blockIdx.y];
+  int bad = 0;
+  for (int r0 = blockIdx.x * 32; r0 < o.brows; r0 += gridDim.x * 32) {  // block-uniform
+    const int row = r0 + (int)(threadIdx.x >> 3);
+    const int lane = threadIdx.x & 7;
+    if (row < o.brows) {
+      const int s0 = o.brpt[row], s1 = o.brpt[row + 1];
+      for (int e = s0 + lane; e + 1 < s1; e += 8) bad |= (o.bcol[e] >= o.bcol[e + 1]);
+    }
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags, B_UNSORTED);
+}
+
+cudaError_t launch_check_sorted_table(const Operands<void> *ops, int nprod, int max_brows,
+                                      int *flags, cudaStream_t s) {
+  if (nprod <= 0 || max_brows <= 0) return cudaSuccess;
+  const int gx = (int)std::min<int64_t>(((int64_t)max_brows + 31) / 32, 1024);
+  k_check_sorted_table<<<dim3(gx, nprod), 256, 0, s>>>(ops, flags);
+  return cudaGetLastError();
+}
+
 // ---- intermediate products and symbolic bins ---------------------------------
 // A rows longer than this are counted by a whole block (k_rowinfo_long), so
 // a power-law row of 10^4 entries does not leave one lane group walking it.
@@ -46,8 +70,7 @@ constexpr int kRowinfoLong = 1024;
 
 template <int GA>
 __global__ void __launch_bounds__(256)
-    k_rowinfo(const int *__restrict__ arpt, const int *__restrict__ acol,
-              const int *__restrict__ brpt, int n, int ncols_b,
+    k_rowinfo(const ProdTable<void> src, int n,
               int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
               int *__restrict__ sym_counts,
               unsigned long long *__restrict__ total_ip, int *__restrict__ flags,
@@ -69,22 +92,24 @@ __global__ void __launch_bounds__(256)
   int bad = 0;
   for (int row = blockIdx.x * kGroups + (int)threadIdx.x / GA; row < n;
        row += gridDim.x * kGroups) {
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<void> o;
+    const int lr = prod_row(src, row, o);
+    const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     if (long_list && a1 - a0 > kRowinfoLong) {  // left to k_rowinfo_long
       if (lane == 0) long_list[atomicAdd(long_count, 1)] = row;
       continue;
     }
     long long ip = 0;
     for (int j = a0 + lane; j < a1; j += GA) {
-      const int k = ld_stream(acol + j);
-      ip += brpt[k + 1] - brpt[k];
+      const int k = ld_stream(o.acol + j);
+      ip += o.brpt[k + 1] - o.brpt[k];
       // each entry against its predecessor, read directly: no dependence
       // between rounds, so long rows keep their loads in flight
-      if (flags && j > a0 && k <= __ldg(acol + j - 1)) bad = 1;
+      if (flags && j > a0 && k <= __ldg(o.acol + j - 1)) bad = 1;
     }
     ip = cg::reduce(tile, ip, cg::plus<long long>());
     if (lane == 0) {
-      const int ub = (int)(ip < (long long)ncols_b ? ip : (long long)ncols_b);
+      const int ub = (int)(ip < (long long)o.ncols ? ip : (long long)o.ncols);
       row_nz[row] = ub;
       if (row_ip) row_ip[row] = ip;
       if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
@@ -100,8 +125,7 @@ __global__ void __launch_bounds__(256)
 
 // The rows k_rowinfo listed: one block per row, the same outputs.
 __global__ void __launch_bounds__(256)
-    k_rowinfo_long(const int *__restrict__ arpt, const int *__restrict__ acol,
-                   const int *__restrict__ brpt, int ncols_b, const int *__restrict__ long_list,
+    k_rowinfo_long(const ProdTable<void> src, const int *__restrict__ long_list,
                    const int *__restrict__ long_count, int *__restrict__ row_nz,
                    int64_t *__restrict__ row_ip, int *__restrict__ sym_counts,
                    unsigned long long *__restrict__ total_ip, int *__restrict__ flags) {
@@ -116,12 +140,14 @@ __global__ void __launch_bounds__(256)
   int bad = 0;
   for (int q = blockIdx.x; q < count; q += gridDim.x) {  // uniform across the block
     const int row = long_list[q];
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<void> o;
+    const int lr = prod_row(src, row, o);
+    const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     long long ip = 0;
     for (int j = a0 + (int)threadIdx.x; j < a1; j += 256) {
-      const int k = ld_stream(acol + j);
-      ip += brpt[k + 1] - brpt[k];
-      if (flags && j > a0 && k <= __ldg(acol + j - 1)) bad = 1;
+      const int k = ld_stream(o.acol + j);
+      ip += o.brpt[k + 1] - o.brpt[k];
+      if (flags && j > a0 && k <= __ldg(o.acol + j - 1)) bad = 1;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ip += __shfl_xor_sync(0xffffffffu, ip, o);
@@ -130,7 +156,7 @@ __global__ void __launch_bounds__(256)
     if (threadIdx.x == 0) {
       long long t = 0;
       for (int w = 0; w < 8; ++w) t += red[w];
-      const int ub = (int)(t < (long long)ncols_b ? t : (long long)ncols_b);
+      const int ub = (int)(t < (long long)o.ncols ? t : (long long)o.ncols);
       row_nz[row] = ub;
       if (row_ip) row_ip[row] = t;
       if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
@@ -144,27 +170,25 @@ __global__ void __launch_bounds__(256)
   if (threadIdx.x == 0 && s_total) atomicAdd(total_ip, s_total);
 }
 
-cudaError_t launch_rowinfo(const CsrDev &A, const CsrDev &B, int *row_nz,
+cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *row_nz,
                            int64_t *row_ip, int *sym_counts,
                            unsigned long long *total_ip, int *flags, int *long_list,
                            int *long_count, cudaStream_t s) {
-  const int n = A.nrows;
   if (n <= 0) return cudaSuccess;
-  const double avg = (double)A.nnz / (double)n;
+  const double avg = (double)a_nnz / (double)n;
   const int ga = avg > 24.0 ? 32 : avg > 12.0 ? 16 : avg > 6.0 ? 8 : 4;
   const int grid = (int)std::min<int64_t>(((int64_t)n * ga + 255) / 256,
                                           (int64_t)dev_info().sms * 8);
   switch (ga) {
-    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
-    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
-    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
-    default: k_rowinfo<4><<<grid, 256, 0, s>>>(A.rpt, A.col, B.rpt, n, B.ncols, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    default: k_rowinfo<4><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !long_list) return e;
-  k_rowinfo_long<<<dev_info().sms * 4, 256, 0, s>>>(A.rpt, A.col, B.rpt, B.ncols, long_list,
-                                                     long_count, row_nz, row_ip, sym_counts,
-                                                     total_ip, flags);
+  k_rowinfo_long<<<dev_info().sms * 4, 256, 0, s>>>(t, long_list, long_count, row_nz, row_ip,
+                                                     sym_counts, total_ip, flags);
   return cudaGetLastError();
 }
 

@@ -145,6 +145,14 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   fill(A, a);
   fill(B, b);
   n = A.nrows;
+  t64 = ProdTable<double>{};
+  t64.one = Operands<double>{A.rpt, A.col, A.val, B.rpt, B.col, B.val, B.ncols, B.nrows};
+  t32 = ProdTable<float>{};
+  t32.one = Operands<float>{A.rpt, A.col, A.val32, B.rpt, B.col, B.val32, B.ncols, B.nrows};
+  info = ProdInfo{n, B.ncols, 1, B.nrows};
+  a_nnz = A.nnz;
+  table = false;
+  ops = nullptr;
   if (opts.timing) {
     timing = true;
     for (auto &e : ev) cudaEventCreate(&e);
@@ -157,6 +165,23 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
     lanes = pick_lanes(avg, A.nrows);
   }
   return NSPB_OK;
+}
+
+void Call::set_table(const ProdTable<double> &d, const ProdTable<float> &f, const ProdInfo &pi,
+                     int64_t total_a_nnz) {
+  t64 = d;
+  t32 = f;
+  info = pi;
+  n = pi.n;
+  a_nnz = total_a_nnz;
+  table = true;
+  ops = reinterpret_cast<const Operands<void> *>(d.ops);
+  A = CsrDev{};
+  B = CsrDev{};
+  A.nrows = pi.n;
+  A.nnz = total_a_nnz;
+  B.ncols = pi.max_ncols;
+  if (!(opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32)) lanes = 32;
 }
 
 size_t Call::scratch_bytes() {
@@ -256,13 +281,17 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   if (st) return st;
   mark(0);
   // B = A (the same arrays): the row walk of k_rowinfo checks B's order too
-  const bool same = A.rpt == B.rpt && A.col == B.col && A.nrows == B.nrows && A.nnz == B.nnz;
+  const bool same = !table && A.rpt == B.rpt && A.col == B.col && A.nrows == B.nrows &&
+                    A.nnz == B.nnz;
   if (!opts.assume_sorted && !same) {
-    if ((e = launch_check_sorted(B, &ctr->flags, s)) != cudaSuccess) return cuda_fail(e);
+    e = table ? launch_check_sorted_table(ops, info.nprod, info.max_brows, &ctr->flags, s)
+              : launch_check_sorted(B, &ctr->flags, s);
+    if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
   // perm is free until the bins are permuted: it holds the long-row list here
-  if ((e = launch_rowinfo(A, B, row_nz, nullptr, ctr->sym_counts, &ctr->total_ip,
+  if ((e = launch_rowinfo(structure_of(t64), n, a_nnz, row_nz, nullptr, ctr->sym_counts,
+                          &ctr->total_ip,
                           !opts.assume_sorted && same ? &ctr->flags : nullptr, perm,
                           &ctr->long_rows, s)) != cudaSuccess)
     return cuda_fail(e);
@@ -273,8 +302,8 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   intprod = (int64_t)h.total_ip;
   // the mean length of the B rows actually read, weighted by how often A reads
   // them: a block-diagonal batch mixes products whose B rows differ
-  if (!(opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32) && A.nnz > 0)
-    lanes = pick_lanes((double)intprod / (double)A.nnz, n);
+  if (!(opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32) && a_nnz > 0)
+    lanes = pick_lanes((double)intprod / (double)a_nnz, n);
   int nonempty = 0, binned = 0;
   BinOffsets off = offsets_of(h.sym_counts, kSymBins, &nonempty, &binned);
   const bool direct = nonempty == 1 && binned == n;
@@ -290,8 +319,8 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     const int c = h.sym_counts[b];
     if (c <= 0) continue;
     const int *rows = direct ? nullptr : perm + off.v[b];
-    e = launch_symbolic_bin(b, lanes, b_sorted, A, B, rows, c, row_nz, &ctr->err,
-                            &ctr->ticket[b], s);
+    e = launch_symbolic_bin(b, lanes, b_sorted, structure_of(t64), info, rows, c, row_nz,
+                            &ctr->err, &ctr->ticket[b], s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
   }
@@ -337,18 +366,21 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
     if (b < kNumGroupBins && b_sorted && staged) {
       const int rg_shift = (opts.row_kernel & 0xff) == 3 ? -1 : 0;  // tables 2x, else 4x
-      e = comp ? launch_numeric_comp_rg(b, lanes, rg_shift, rg_depth(), A, B, crpt, ccol, cval, rows, c, nmax,
-                                        &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
-               : launch_numeric_rg(b, lanes, rg_shift, rg_depth(), A, B, crpt, ccol, cval, rows, c,
-                                   &ctr->err, s);
+      e = comp ? launch_numeric_comp_rg(b, lanes, rg_shift, rg_depth(), t32, crpt, ccol, cval,
+                                        rows, c, nmax, &ctr->redo_count, &ctr->max_comp_deg,
+                                        &ctr->err, s)
+               : launch_numeric_rg(b, lanes, rg_shift, rg_depth(), t64, crpt, ccol, cval, rows,
+                                   c, &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;
       continue;
     }
-    e = comp ? launch_numeric_comp_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows,
+    e = comp ? launch_numeric_comp_bin(b, lanes, b_sorted, b_sorted, t32, info, crpt, ccol, cval,
+                                       rows,
                                        c, nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err,
                                        ticket, tshift, s)
-             : launch_numeric_bin(b, lanes, b_sorted, b_sorted, A, B, crpt, ccol, cval, rows, c,
+             : launch_numeric_bin(b, lanes, b_sorted, b_sorted, t64, info, crpt, ccol, cval,
+                                  rows, c,
                                   &ctr->err, ticket, tshift, s);
     if (e != cudaSuccess) return cuda_fail(e);
     ++launches;
@@ -363,8 +395,11 @@ int Call::prepare_numeric(const int *crpt) {
   int st = alloc_scratch();
   if (st) return st;
   cudaError_t e;
-  if (!opts.assume_sorted && (e = launch_check_sorted(B, &ctr->flags, s)) != cudaSuccess)
-    return cuda_fail(e);
+  if (!opts.assume_sorted) {
+    e = table ? launch_check_sorted_table(ops, info.nprod, info.max_brows, &ctr->flags, s)
+              : launch_check_sorted(B, &ctr->flags, s);
+    if (e != cudaSuccess) return cuda_fail(e);
+  }
   if ((e = launch_num_hist(crpt, n, ctr->num_counts, s)) != cudaSuccess) return cuda_fail(e);
   launches += opts.assume_sorted ? 1 : 2;
   if ((st = fetch_counters())) return st;
@@ -619,7 +654,8 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip, 
     return NSPB_OK;
   }
   if ((st = call.alloc_scratch())) return st;
-  cudaError_t e = launch_rowinfo(call.A, call.B, call.row_nz, d_row_ip, call.ctr->sym_counts,
+  cudaError_t e = launch_rowinfo(structure_of(call.t64), call.n, call.a_nnz, call.row_nz,
+                                 d_row_ip, call.ctr->sym_counts,
                                  &call.ctr->total_ip, nullptr, call.perm, &call.ctr->long_rows,
                                  call.s);
   if (e != cudaSuccess) return call.cuda_fail(e);

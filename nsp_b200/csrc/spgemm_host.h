@@ -42,7 +42,14 @@ int alloc_out(void **p, size_t bytes);
 struct Call {
   nspb_opts opts{};
   cudaStream_t s = nullptr;
-  CsrDev A, B;
+  CsrDev A, B;  // one product's operands (a table of one); see set_table for batches
+  // what the kernels read: one product by value, or a device table of products
+  ProdTable<double> t64;
+  ProdTable<float> t32;
+  ProdInfo info;
+  int64_t a_nnz = 0;                // entries of A over all products
+  bool table = false;               // several products through a device table
+  const Operands<void> *ops = nullptr;
   int n = 0;
   int lanes = 32;
   // scratch (one stream-ordered block)
@@ -87,6 +94,10 @@ struct Call {
   }
 
   int init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o);
+  // Batched call: the products of a device table instead of init's A and B
+  // (init must have run with any valid operands first; opts are kept).
+  void set_table(const ProdTable<double> &d, const ProdTable<float> &f, const ProdInfo &pi,
+                 int64_t total_a_nnz);
   size_t scratch_bytes();  // sets the scratch offsets; bytes alloc_scratch needs
   int alloc_scratch();
   int cuda_fail(cudaError_t e);

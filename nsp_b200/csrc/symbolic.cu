@@ -32,10 +32,8 @@ struct SymGroupCfg {
 
 template <int G, int LOG2T>
 __global__ void __launch_bounds__(256)
-    k_sym_group(const int *__restrict__ arpt, const int *__restrict__ acol,
-                const int *__restrict__ brpt, const int *__restrict__ bcol,
-                const int *__restrict__ rows, int count, int *__restrict__ row_nz,
-                int *__restrict__ err) {
+    k_sym_group(const ProdTable<void> src, const int *__restrict__ rows, int count,
+                int *__restrict__ row_nz, int *__restrict__ err) {
   using C = SymGroupCfg<G, LOG2T>;
   extern __shared__ __align__(16) int smem_sym[];
   auto tile = cg::tiled_partition<G>(cg::this_thread_block());
@@ -49,21 +47,23 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 4
     for (int s = lane; s < C::T / 4; s += G) t4[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
     tile.sync();
-    const int a0 = arpt[row], a1 = arpt[row + 1];
+    Operands<void> o;
+    const int lr = prod_row(src, row, o);
+    const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     int nz = 0;
     for (int ab = a0; ab < a1; ab += G) {
       // lanes fetch up to G A entries and their B row bounds at once
       int bs = 0, be = 0;
       if (ab + lane < a1) {
-        const int k = ld_stream(acol + ab + lane);
-        bs = __ldg(brpt + k);
-        be = __ldg(brpt + k + 1);
+        const int k = ld_stream(o.acol + ab + lane);
+        bs = __ldg(o.brpt + k);
+        be = __ldg(o.brpt + k + 1);
       }
       const int cnt = min(G, a1 - ab);
       for (int t = 0; t < cnt; ++t) {
         const int s0 = tile.shfl(bs, t), s1 = tile.shfl(be, t);
         for (int e = s0 + lane; e < s1; e += G)
-          nz += sym_insert<LOG2T>(table, __ldg(bcol + e), err);
+          nz += sym_insert<LOG2T>(table, __ldg(o.bcol + e), err);
       }
     }
     nz = cg::reduce(tile, nz, cg::plus<int>());
@@ -89,9 +89,7 @@ constexpr int kWideHashMax = 3 << (kWideLog2T - 2);
 // 145 KB of shared memory a block: one block per SM, so the minimum of one
 // block lets ptxas use 64 registers a thread (it kept 32 without it)
 __global__ void __launch_bounds__(kWideThreads, 1)
-    k_sym_wide(const int *__restrict__ arpt, const int *__restrict__ acol,
-               const int *__restrict__ brpt, const int *__restrict__ bcol, int ncols,
-               int b_sorted, const int *__restrict__ rows, int count,
+    k_sym_wide(const ProdTable<void> src, int b_sorted, const int *__restrict__ rows, int count,
                int *__restrict__ row_nz, int *__restrict__ err, int *__restrict__ ticket) {
   extern __shared__ __align__(16) unsigned bm[];
   __shared__ int red[kWideThreads / 32];
@@ -115,8 +113,12 @@ __global__ void __launch_bounds__(kWideThreads, 1)
   };
   for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
-    const int a0 = arpt[row], a1 = arpt[row + 1];
-    const RowSpan sp = row_span<kWideThreads>(acol, brpt, bcol, a0, a1, b_sorted != 0, ncols, sc);
+    Operands<void> o;
+    const int lr = prod_row(src, row, o);
+    const int *acol = o.acol, *brpt = o.brpt, *bcol = o.bcol;
+    const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
+    const RowSpan sp = row_span<kWideThreads>(acol, brpt, bcol, a0, a1, b_sorted != 0, o.ncols,
+                                              sc);
     int total = 0;
     if ((long long)sp.hi - sp.lo + 1 > kLongBits && sp.ip <= kWideHashMax) {
       int *table = reinterpret_cast<int *>(bm);
@@ -157,49 +159,47 @@ __global__ void __launch_bounds__(kWideThreads, 1)
 
 // ---- dispatch -------------------------------------------------------------------
 template <int G, int LOG2T>
-static cudaError_t run_sym_group(const CsrDev &A, const CsrDev &B, const int *rows,
-                                 int count, int *row_nz, int *err, cudaStream_t s) {
+static cudaError_t run_sym_group(const ProdTable<void> &t, const int *rows, int count,
+                                 int *row_nz, int *err, cudaStream_t s) {
   using C = SymGroupCfg<G, LOG2T>;
   const void *f = (const void *)k_sym_group<G, LOG2T>;
   const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_group<G, LOG2T><<<grid, C::THREADS, C::SMEM, s>>>(A.rpt, A.col, B.rpt, B.col, rows,
-                                                          count, row_nz, err);
+  k_sym_group<G, LOG2T><<<grid, C::THREADS, C::SMEM, s>>>(t, rows, count, row_nz, err);
   return cudaGetLastError();
 }
 
 template <int G>
-static cudaError_t sym_group_bin(int bin, const CsrDev &A, const CsrDev &B, const int *rows,
-                                 int count, int *row_nz, int *err, cudaStream_t s) {
+static cudaError_t sym_group_bin(int bin, const ProdTable<void> &t, const int *rows, int count,
+                                 int *row_nz, int *err, cudaStream_t s) {
   switch (bin) {
-    case 0: return run_sym_group<G, 5>(A, B, rows, count, row_nz, err, s);
-    case 1: return run_sym_group<G, 6>(A, B, rows, count, row_nz, err, s);
-    case 2: return run_sym_group<G, 7>(A, B, rows, count, row_nz, err, s);
-    case 3: return run_sym_group<G, 8>(A, B, rows, count, row_nz, err, s);
-    case 4: return run_sym_group<G, 9>(A, B, rows, count, row_nz, err, s);
-    case 5: return run_sym_group<G, 10>(A, B, rows, count, row_nz, err, s);
-    case 6: return run_sym_group<G, 11>(A, B, rows, count, row_nz, err, s);
-    default: return run_sym_group<G, 12>(A, B, rows, count, row_nz, err, s);
+    case 0: return run_sym_group<G, 5>(t, rows, count, row_nz, err, s);
+    case 1: return run_sym_group<G, 6>(t, rows, count, row_nz, err, s);
+    case 2: return run_sym_group<G, 7>(t, rows, count, row_nz, err, s);
+    case 3: return run_sym_group<G, 8>(t, rows, count, row_nz, err, s);
+    case 4: return run_sym_group<G, 9>(t, rows, count, row_nz, err, s);
+    case 5: return run_sym_group<G, 10>(t, rows, count, row_nz, err, s);
+    case 6: return run_sym_group<G, 11>(t, rows, count, row_nz, err, s);
+    default: return run_sym_group<G, 12>(t, rows, count, row_nz, err, s);
   }
 }
 
-cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const CsrDev &A,
-                                const CsrDev &B, const int *rows, int count, int *row_nz,
+cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTable<void> &t,
+                                const ProdInfo &info, const int *rows, int count, int *row_nz,
                                 int *err, int *ticket, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin < kSymGroupBins) {
-    if (lanes == 8) return sym_group_bin<8>(bin, A, B, rows, count, row_nz, err, s);
-    if (lanes == 16) return sym_group_bin<16>(bin, A, B, rows, count, row_nz, err, s);
-    return sym_group_bin<32>(bin, A, B, rows, count, row_nz, err, s);
+    if (lanes == 8) return sym_group_bin<8>(bin, t, rows, count, row_nz, err, s);
+    if (lanes == 16) return sym_group_bin<16>(bin, t, rows, count, row_nz, err, s);
+    return sym_group_bin<32>(bin, t, rows, count, row_nz, err, s);
   }
   // the bitmap covers one window of B's columns at most; the hash table needs
   // the full 128 KB, which it only uses when B has more columns than a window
-  const int smem = (int)std::min<long long>(kLongWords, ((long long)B.ncols + 31) >> 5) * 4;
+  const int smem = (int)std::min<long long>(kLongWords, ((long long)info.max_ncols + 31) >> 5) * 4;
   const void *f = (const void *)k_sym_wide;
   const int grid = persistent_grid(f, kWideThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_wide<<<grid, kWideThreads, smem, s>>>(A.rpt, A.col, B.rpt, B.col, B.ncols,
-                                              b_sorted ? 1 : 0, rows, count, row_nz, err,
+  k_sym_wide<<<grid, kWideThreads, smem, s>>>(t, b_sorted ? 1 : 0, rows, count, row_nz, err,
                                               ticket);
   return cudaGetLastError();
 }
