@@ -18,15 +18,18 @@ namespace nspb {
 // ---- operands of a row ---------------------------------------------------------
 // The operands of global row r of a call and the row's index inside its
 // product (see ProdTable in internal.h).
-template <typename VT>
+// MULTI false: one product, whose pointers stay kernel parameters (no
+// registers held for them across the row); true: a table of products.
+template <bool MULTI, typename VT>
 __device__ __forceinline__ int prod_row(const ProdTable<VT> &t, int r, Operands<VT> &o) {
-  if (!t.prod_of_row) {
+  if constexpr (!MULTI) {
     o = t.one;
     return r;
+  } else {
+    const int p = __ldg(t.prod_of_row + r);
+    o = t.ops[p];
+    return r - __ldg(t.row_off + p);
   }
-  const int p = __ldg(t.prod_of_row + r);
-  o = t.ops[p];
-  return r - __ldg(t.row_off + p);
 }
 
 // ---- error word bits (device -> host) ---------------------------------------

@@ -64,7 +64,7 @@ struct NumGroupCfg {
 
 // VT: value type of A and B (double, or float in the compensated mode).
 // COMP: fp32 inputs with the error-free pair accumulation for short rows.
-template <int G, int LOG2T, bool OWNED, typename VT, bool COMP>
+template <int G, int LOG2T, bool OWNED, typename VT, bool COMP, bool MULTI>
 __global__ void __launch_bounds__(256)
     k_num_group(const ProdTable<VT> src, const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256)
       reinterpret_cast<int4 *>(keys)[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
     tile.sync();
     Operands<VT> op;
-    const int lr = prod_row(src, row, op);
+    const int lr = prod_row<MULTI>(src, row, op);
     const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
     const VT *aval = op.aval, *bval = op.bval;
     const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
@@ -280,7 +280,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *red, int *tot) {
   return r;
 }
 
-template <int LOG2T, typename VT>
+template <int LOG2T, typename VT, bool MULTI>
 __global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
     k_num_block(const ProdTable<VT> src, const int *__restrict__ crpt, int *__restrict__ ccol,
                 double *__restrict__ cval, const int *__restrict__ rows, int count,
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kNumBlockThreads, num_block_minb(LOG2T))
     }
     __syncthreads();
     Operands<VT> op;
-    const int lr = prod_row(src, row, op);
+    const int lr = prod_row<MULTI>(src, row, op);
     const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     int mn = 0x7fffffff, mx = -1;
     row_products<kNumBlockThreads>(op.acol, op.aval, op.brpt, op.bcol, op.bval, a0, a1, rq,
@@ -451,7 +451,7 @@ __device__ __forceinline__ void red_add_global_keep(double *p, double v, unsigne
                : "memory");
 }
 
-template <typename VT, int MINB>
+template <typename VT, int MINB, bool MULTI>
 __global__ void __launch_bounds__(kRankThreads, MINB)
     k_num_rank(const ProdTable<VT> src, int b_sorted, int pl_max, const int *__restrict__ crpt,
                int *__restrict__ ccol, double *__restrict__ cval,
@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(kRankThreads, MINB)
   for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
     Operands<VT> op;
-    const int lr = prod_row(src, row, op);
+    const int lr = prod_row<MULTI>(src, row, op);
     const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
     const VT *aval = op.aval, *bval = op.bval;
     const int ncols = op.ncols;
@@ -595,7 +595,9 @@ static cudaError_t run_num_rank(const ProdTable<VT> &t, const ProdInfo &info, bo
                                 int count, int *err, int *redo, int *ticket, cudaStream_t s) {
   const int pl = rank_per_log2((int)std::min<long long>(info.max_ncols, kRankMaxCols));
   const int smem = rank_smem(pl);
-  auto kern = rank_minb(pl) == 1 ? k_num_rank<VT, 1> : k_num_rank<VT, 2>;
+  const bool multi = t.prod_of_row != nullptr;
+  auto kern = rank_minb(pl) == 1 ? (multi ? k_num_rank<VT, 1, true> : k_num_rank<VT, 1, false>)
+                                 : (multi ? k_num_rank<VT, 2, true> : k_num_rank<VT, 2, false>);
   const int grid = persistent_grid((const void *)kern, kRankThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, kRankThreads, smem, s>>>(t, b_sorted ? 1 : 0, pl, crpt, ccol, cval, rows, count,
@@ -609,11 +611,11 @@ static cudaError_t run_num_group(const ProdTable<VT> &t, const int *crpt, int *c
                                  double *cval, const int *rows, int count, int *err,
                                  CompArgs comp, cudaStream_t s) {
   using C = NumGroupCfg<G, LOG2T>;
-  const void *f = (const void *)k_num_group<G, LOG2T, OWNED, VT, COMP>;
-  const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
+  auto kern = t.prod_of_row ? k_num_group<G, LOG2T, OWNED, VT, COMP, true>
+                            : k_num_group<G, LOG2T, OWNED, VT, COMP, false>;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_group<G, LOG2T, OWNED, VT, COMP><<<grid, C::THREADS, C::SMEM, s>>>(
-      t, crpt, ccol, cval, rows, count, err, comp);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, crpt, ccol, cval, rows, count, err, comp);
   return cudaGetLastError();
 }
 
@@ -642,11 +644,10 @@ static cudaError_t run_num_block(const ProdTable<VT> &t, const int *crpt, int *c
                                  int *ticket, cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
   const int smem = T * 12 + (T / 2) * 12 + (T / 2) * 4;
-  const void *f = (const void *)k_num_block<LOG2T, VT>;
-  const int grid = persistent_grid(f, kNumBlockThreads, smem, count, 1);
+  auto kern = t.prod_of_row ? k_num_block<LOG2T, VT, true> : k_num_block<LOG2T, VT, false>;
+  const int grid = persistent_grid((const void *)kern, kNumBlockThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_num_block<LOG2T, VT><<<grid, kNumBlockThreads, smem, s>>>(t, crpt, ccol, cval, rows, count,
-                                                               err, redo, ticket);
+  kern<<<grid, kNumBlockThreads, smem, s>>>(t, crpt, ccol, cval, rows, count, err, redo, ticket);
   return cudaGetLastError();
 }
 

@@ -68,7 +68,7 @@ cudaError_t launch_check_sorted_table(const Operands<void> *ops, int nprod, int 
 // a power-law row of 10^4 entries does not leave one lane group walking it.
 constexpr int kRowinfoLong = 1024;
 
-template <int GA>
+template <int GA, bool MULTI>
 __global__ void __launch_bounds__(256)
     k_rowinfo(const ProdTable<void> src, int n,
               int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256)
   for (int row = blockIdx.x * kGroups + (int)threadIdx.x / GA; row < n;
        row += gridDim.x * kGroups) {
     Operands<void> o;
-    const int lr = prod_row(src, row, o);
+    const int lr = prod_row<MULTI>(src, row, o);
     const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     if (long_list && a1 - a0 > kRowinfoLong) {  // left to k_rowinfo_long
       if (lane == 0) long_list[atomicAdd(long_count, 1)] = row;
@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // The rows k_rowinfo listed: one block per row, the same outputs.
+template <bool MULTI>
 __global__ void __launch_bounds__(256)
     k_rowinfo_long(const ProdTable<void> src, const int *__restrict__ long_list,
                    const int *__restrict__ long_count, int *__restrict__ row_nz,
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(256)
   for (int q = blockIdx.x; q < count; q += gridDim.x) {  // uniform across the block
     const int row = long_list[q];
     Operands<void> o;
-    const int lr = prod_row(src, row, o);
+    const int lr = prod_row<MULTI>(src, row, o);
     const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     long long ip = 0;
     for (int j = a0 + (int)threadIdx.x; j < a1; j += 256) {
@@ -179,16 +180,24 @@ cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *
   const int ga = avg > 24.0 ? 32 : avg > 12.0 ? 16 : avg > 6.0 ? 8 : 4;
   const int grid = (int)std::min<int64_t>(((int64_t)n * ga + 255) / 256,
                                           (int64_t)dev_info().sms * 8);
+  const bool multi = t.prod_of_row != nullptr;
+#define NSPB_RI(GA)                                                                         \
+  (multi ? k_rowinfo<GA, true><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, \
+                                                    flags, long_list, long_count)           \
+         : k_rowinfo<GA, false><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts,       \
+                                                     total_ip, flags, long_list, long_count))
   switch (ga) {
-    case 32: k_rowinfo<32><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
-    case 16: k_rowinfo<16><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
-    case 8: k_rowinfo<8><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
-    default: k_rowinfo<4><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, flags, long_list, long_count); break;
+    case 32: NSPB_RI(32); break;
+    case 16: NSPB_RI(16); break;
+    case 8: NSPB_RI(8); break;
+    default: NSPB_RI(4); break;
   }
+#undef NSPB_RI
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !long_list) return e;
-  k_rowinfo_long<<<dev_info().sms * 4, 256, 0, s>>>(t, long_list, long_count, row_nz, row_ip,
-                                                     sym_counts, total_ip, flags);
+  auto klong = multi ? k_rowinfo_long<true> : k_rowinfo_long<false>;
+  klong<<<dev_info().sms * 4, 256, 0, s>>>(t, long_list, long_count, row_nz, row_ip, sym_counts,
+                                           total_ip, flags);
   return cudaGetLastError();
 }
 

@@ -30,7 +30,7 @@ struct SymGroupCfg {
   static constexpr int SMEM = GPC * T * 4;
 };
 
-template <int G, int LOG2T>
+template <int G, int LOG2T, bool MULTI>
 __global__ void __launch_bounds__(256)
     k_sym_group(const ProdTable<void> src, const int *__restrict__ rows, int count,
                 int *__restrict__ row_nz, int *__restrict__ err) {
@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(256)
     for (int s = lane; s < C::T / 4; s += G) t4[s] = make_int4(kEmpty, kEmpty, kEmpty, kEmpty);
     tile.sync();
     Operands<void> o;
-    const int lr = prod_row(src, row, o);
+    const int lr = prod_row<MULTI>(src, row, o);
     const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     int nz = 0;
     for (int ab = a0; ab < a1; ab += G) {
@@ -88,6 +88,7 @@ constexpr int kWideHashMax = 3 << (kWideLog2T - 2);
 
 // 145 KB of shared memory a block: one block per SM, so the minimum of one
 // block lets ptxas use 64 registers a thread (it kept 32 without it)
+template <bool MULTI>
 __global__ void __launch_bounds__(kWideThreads, 1)
     k_sym_wide(const ProdTable<void> src, int b_sorted, const int *__restrict__ rows, int count,
                int *__restrict__ row_nz, int *__restrict__ err, int *__restrict__ ticket) {
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(kWideThreads, 1)
   for (int r = next_row(ticket, count, &s_slot); r < count; r = next_row(ticket, count, &s_slot)) {
     const int row = rows ? rows[r] : r;
     Operands<void> o;
-    const int lr = prod_row(src, row, o);
+    const int lr = prod_row<MULTI>(src, row, o);
     const int *acol = o.acol, *brpt = o.brpt, *bcol = o.bcol;
     const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
     const RowSpan sp = row_span<kWideThreads>(acol, brpt, bcol, a0, a1, b_sorted != 0, o.ncols,
@@ -162,10 +163,10 @@ template <int G, int LOG2T>
 static cudaError_t run_sym_group(const ProdTable<void> &t, const int *rows, int count,
                                  int *row_nz, int *err, cudaStream_t s) {
   using C = SymGroupCfg<G, LOG2T>;
-  const void *f = (const void *)k_sym_group<G, LOG2T>;
-  const int grid = persistent_grid(f, C::THREADS, C::SMEM, count, C::GPC);
+  auto kern = t.prod_of_row ? k_sym_group<G, LOG2T, true> : k_sym_group<G, LOG2T, false>;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_group<G, LOG2T><<<grid, C::THREADS, C::SMEM, s>>>(t, rows, count, row_nz, err);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, rows, count, row_nz, err);
   return cudaGetLastError();
 }
 
@@ -196,11 +197,10 @@ cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTab
   // the bitmap covers one window of B's columns at most; the hash table needs
   // the full 128 KB, which it only uses when B has more columns than a window
   const int smem = (int)std::min<long long>(kLongWords, ((long long)info.max_ncols + 31) >> 5) * 4;
-  const void *f = (const void *)k_sym_wide;
-  const int grid = persistent_grid(f, kWideThreads, smem, count, 1);
+  auto kern = t.prod_of_row ? k_sym_wide<true> : k_sym_wide<false>;
+  const int grid = persistent_grid((const void *)kern, kWideThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  k_sym_wide<<<grid, kWideThreads, smem, s>>>(t, b_sorted ? 1 : 0, rows, count, row_nz, err,
-                                              ticket);
+  kern<<<grid, kWideThreads, smem, s>>>(t, b_sorted ? 1 : 0, rows, count, row_nz, err, ticket);
   return cudaGetLastError();
 }
 
