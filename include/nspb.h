@@ -121,8 +121,14 @@ typedef struct {
                             of C), else hash tables with an in-table sort;
                             1 = always the hash-sort kernels; 2 = always the
                             staged walk (tables of 4x the bin's row limit);
-                            3 = staged walk with tables of 2x. Bits 8-15:
-                            B rows the staged walk loads ahead (0 = 4)       */
+                            3 = staged walk with tables of 2x              */
+  int32_t sym_fill_pct;  /* symbolic bin thresholds: a row goes to the bin
+                            whose table (32 << b slots) it fills to at most
+                            this percentage at its upper bound of distinct
+                            columns; 0 = 75, else 10..90                     */
+  int32_t num_fill_pct;  /* numeric bin thresholds: a row of nnz entries goes
+                            to the bin whose 32 << b slots it fills to at
+                            most this percentage; 0 = 50, else 10..50        */
 } nspb_opts;
 
 /* Per-call figures (all optional; pass NULL).                               */
@@ -220,17 +226,23 @@ int nspb_spgemm_host(const nspb_csr_in *hA, const nspb_csr_in *hB, int32_t *h_ro
                      int32_t nblocks, const nspb_opts *opts);
 
 /* ---- autotuner ---------------------------------------------------------------
- * Times this product (C sized once, then written into the same arrays) with
- * every candidate of threads per row (group_lanes 8, 16, 32) and numeric
- * table size (num_table_shift 0, 1): one warm-up and `reps` timed calls each,
+ * Times this product (C sized once, then written into the same arrays) under
+ * candidates of the row-group threads per row (group_lanes 8, 16, 32), kernel
+ * family (row_kernel 1 hash-sort, 2 staged walk), table size (num_table_shift
+ * 0/1, or row_kernel 2/3) and bin thresholds (sym_fill_pct 50/75/90,
+ * num_fill_pct 25/37/50), each knob swept in turn with the best values found
+ * so far for the others: one warm-up and `reps` timed calls per candidate,
  * CUDA events on opts->stream. *best receives `base` with the fastest
- * candidate's knobs; report (may be NULL; room for 6) the candidates and
- * their mean ms, *n_report their number.                                   */
+ * candidate's knobs; report (may be NULL; room for NSPB_TUNE_MAX_REPORT) the
+ * candidates and their mean ms, *n_report their number.                    */
+#define NSPB_TUNE_MAX_REPORT 16
 typedef struct {
   int32_t group_lanes;
   int32_t num_table_shift;
   float ms;
-  int32_t _pad;
+  int32_t row_kernel;
+  int32_t sym_fill_pct;
+  int32_t num_fill_pct;
 } nspb_tune_entry;
 int nspb_autotune(const nspb_csr_in *A, const nspb_csr_in *B, const nspb_opts *base,
                   int reps, nspb_opts *best, nspb_tune_entry *report, int32_t *n_report);

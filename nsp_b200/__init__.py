@@ -73,7 +73,8 @@ def stats_dict(s: Stats) -> dict:
 def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,
            stream=None, check_errors: bool = True, assume_sorted: bool = False,
            group_lanes: int = 0, comp_tol: float = 1e-10, return_stats: bool = False,
-           table_shift: int = 0, row_kernel: int | None = None):
+           table_shift: int = 0, row_kernel: int | None = None, sym_fill_pct: int = 0,
+           num_fill_pct: int = 0):
     """C = A·B on the current CUDA device through nspb_spgemm.
 
     With `out` given, its tensors are used as C's arrays (capacity = their
@@ -82,6 +83,7 @@ def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR |
     prec = _precision(precision)
     o = make_opts(prec, assume_sorted, check_errors, group_lanes, comp_tol, stream, table_shift,
                   row_kernel)
+    o.sym_fill_pct, o.num_fill_pct = int(sym_fill_pct), int(num_fill_pct)
     a, b = A.as_in(), B.as_in()
     c = CsrOut()
     if out is not None:
@@ -136,19 +138,23 @@ def galerkin(A: DeviceCSR, P: DeviceCSR, return_R: bool = False, stream=None):
 
 
 def autotune(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", reps: int = 3, stream=None):
-    """nspb_autotune: ({"group_lanes", "table_shift"} of the fastest candidate,
-    [(group_lanes, table_shift, ms), ...] for every candidate)."""
+    """nspb_autotune: (knobs of the fastest candidate, [(knobs, ms), ...] for
+    every candidate timed). knobs: group_lanes, table_shift, row_kernel,
+    sym_fill_pct, num_fill_pct."""
     from ._lib import TuneEntry
-    prec = _precision(precision)
-    o = make_opts(prec, stream=stream)
+    o = make_opts(_precision(precision), stream=stream)
     best = Opts()
-    rep = (TuneEntry * 6)()
+    rep = (TuneEntry * 16)()
     n = C.c_int32(0)
     a, b = A.as_in(), B.as_in()
     check(lib.nspb_autotune(C.byref(a), C.byref(b), C.byref(o), int(reps), C.byref(best), rep,
                             C.byref(n)), "nspb_autotune")
-    return ({"group_lanes": best.group_lanes, "table_shift": best.num_table_shift},
-            [(rep[i].group_lanes, rep[i].num_table_shift, rep[i].ms) for i in range(n.value)])
+
+    def knobs(x):
+        return {"group_lanes": x.group_lanes, "table_shift": x.num_table_shift,
+                "row_kernel": x.row_kernel, "sym_fill_pct": x.sym_fill_pct,
+                "num_fill_pct": x.num_fill_pct}
+    return knobs(best), [(knobs(rep[i]), rep[i].ms) for i in range(n.value)]
 
 
 def _host_ptr(x):

@@ -55,7 +55,8 @@ class Opts(C.Structure):
                 ("check_errors", C.c_int32), ("group_lanes", C.c_int32),
                 ("timing", C.c_int32), ("batch_max_products", C.c_int32),
                 ("comp_tol", C.c_double), ("stream", C.c_void_p),
-                ("num_table_shift", C.c_int32), ("row_kernel", C.c_int32)]
+                ("num_table_shift", C.c_int32), ("row_kernel", C.c_int32),
+                ("sym_fill_pct", C.c_int32), ("num_fill_pct", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -69,7 +70,8 @@ class Stats(C.Structure):
 
 class TuneEntry(C.Structure):
     _fields_ = [("group_lanes", C.c_int32), ("num_table_shift", C.c_int32),
-                ("ms", C.c_float), ("_pad", C.c_int32)]
+                ("ms", C.c_float), ("row_kernel", C.c_int32), ("sym_fill_pct", C.c_int32),
+                ("num_fill_pct", C.c_int32)]
 
 
 class HostCsr(C.Structure):

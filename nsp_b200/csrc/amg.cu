@@ -219,7 +219,8 @@ int scan_into(const int *in, int n, int *out, Scratch &ws, cudaStream_t s) {
   if (e == cudaSuccess)
     e = cudaMemsetAsync(tiles, 0, (size_t)scan_tiles(n) * sizeof(unsigned long long), s);
   if (e == cudaSuccess)
-    e = launch_scan(in, n, out, &ctr->total, tiles, &ctr->tile_ctr, ctr->num_counts, &ctr->err, s);
+    e = launch_scan(in, n, out, &ctr->total, tiles, &ctr->tile_ctr, bin_limits(0, 0),
+                    ctr->num_counts, &ctr->err, s);
   return cuda_status(e);
 }
 

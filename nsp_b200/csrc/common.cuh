@@ -65,14 +65,15 @@ __host__ __device__ constexpr int sym_limit(int b) {
 __host__ __device__ constexpr int num_limit(int b) {
   return b < kNumLong ? (16 << b) : 0x7fffffff;  // 16,32,...,4096
 }
-__host__ __device__ __forceinline__ int sym_bin(int ub) {
+// Bins under runtime limits (BinLimits, the autotuner's thresholds).
+__host__ __device__ __forceinline__ int sym_bin(int ub, const BinLimits &l) {
   int b = 0;
-  while (b < kSymLong && ub > sym_limit(b)) ++b;
+  while (b < kSymLong && ub > l.sym[b]) ++b;
   return b;
 }
-__host__ __device__ __forceinline__ int num_bin(int nz) {
+__host__ __device__ __forceinline__ int num_bin(int nz, const BinLimits &l) {
   int b = 0;
-  while (b < kNumLong && nz > num_limit(b)) ++b;
+  while (b < kNumLong && nz > l.num[b]) ++b;
   return b;
 }
 

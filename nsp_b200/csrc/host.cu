@@ -122,7 +122,7 @@ int block_numeric(const nspb_csr_in *Ab, const nspb_csr_in *dB, nspb_csr_out *Cb
   if ((st = call.alloc_scratch())) return st;
   for (int r = 0; r < Ab->nrows; ++r) {
     const int len = c_rowptr[r + 1] - c_rowptr[r];
-    if (len > 0) ++call.h.num_counts[num_bin(len)];
+    if (len > 0) ++call.h.num_counts[num_bin_of(len, call.lim)];
   }
   call.b_sorted = ob->assume_sorted != 0;
   call.num_counts_ready = true;

@@ -82,6 +82,18 @@ struct ProdInfo {
   int max_brows = 0;
 };
 
+// Inclusive row limits of the symbolic and numeric bins (the last bin of each
+// is unbounded). The kernel of bin b has a table of 32 << b slots; a limit
+// only moves rows between bins, never past what a bin's kernel holds.
+struct BinLimits {
+  int sym[16];
+  int num[16];
+};
+// From the fill percentages of nspb_opts (0: the defaults, 75% and 50%).
+BinLimits bin_limits(int sym_fill_pct, int num_fill_pct);
+int sym_bin_of(int ub, const BinLimits &l);
+int num_bin_of(int nz, const BinLimits &l);
+
 // Flag bits written by launch_check_sorted.
 enum : int { B_UNSORTED = 1 };
 
@@ -110,7 +122,8 @@ cudaError_t launch_check_sorted_table(const Operands<void> *ops, int nprod, int 
 // would, from the rows read here. long_list / long_count (may be NULL; n ints and
 // a zeroed counter): rows of more than 1024 A entries are listed there and
 // counted by a second kernel, a block per row.
-cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *row_nz,
+cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, const BinLimits &lim,
+                           int *row_nz,
                            int64_t *row_ip, int *sym_counts,
                            unsigned long long *total_ip, int *flags, int *long_list,
                            int *long_count, cudaStream_t s);
@@ -120,7 +133,7 @@ struct BinOffsets {
   int v[16];
 };
 cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets,
-                        int *cursor, int *perm, cudaStream_t s);
+                        const BinLimits &lim, int *cursor, int *perm, cudaStream_t s);
 // Reorder row lists of perm (list i: perm[off[i] .. off[i]+count[i])) so that
 // rows of the heaviest weight class come first; weight as in launch_perm.
 // Lists of more than kOrderCap rows are left as they are.
@@ -137,10 +150,10 @@ cudaError_t launch_order_rows(const int *key, int kind, const RowLists &lists, i
 // scan_tiles(n) entries) and tile_ctr (zeroed).
 int scan_tiles(int n);
 cudaError_t launch_scan(const int *row_nz, int n, int *crpt, long long *total,
-                        unsigned long long *tile_state, int *tile_ctr,
+                        unsigned long long *tile_state, int *tile_ctr, const BinLimits &lim,
                         int *num_counts, int *err, cudaStream_t s);
 // Numeric-bin histogram from an existing row pointer.
-cudaError_t launch_num_hist(const int *crpt, int n, int *num_counts,
+cudaError_t launch_num_hist(const int *crpt, int n, const BinLimits &lim, int *num_counts,
                             cudaStream_t s);
 
 // ---- symbolic.cu ----------------------------------------------------------------

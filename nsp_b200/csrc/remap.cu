@@ -203,7 +203,8 @@ int compactcol_dev(const int *d_in, int64_t n, int lo, int hi, int *d_out, int64
   int st = remap_scratch(r, tiles, 0, s);
   if (st) return st;
   k_tile_count<<<tiles, kCompactThreads, 0, s>>>(d_in, n, lo, hi, r.counts);
-  cudaError_t e = launch_scan(r.counts, tiles, r.offs, r.total, r.tiles, r.hdr_ctr, r.hist, r.err, s);
+  cudaError_t e = launch_scan(r.counts, tiles, r.offs, r.total, r.tiles, r.hdr_ctr, bin_limits(0, 0),
+                                  r.hist, r.err, s);
   if (e == cudaSuccess) {
     k_tile_scatter<<<tiles, kCompactThreads, 0, s>>>(d_in, n, lo, hi, r.offs, d_out);
     e = cudaGetLastError();
@@ -253,7 +254,8 @@ int getmct_dev(const int *d_col, int64_t nnz, int first, int last, int *d_out, i
   cudaMemsetAsync(bm, 0, (size_t)words * 4, s);
   k_set_bits<<<grid_for(nnz, 256), 256, 0, s>>>(d_col, nnz, lo, hi, bm);
   k_word_pop<<<(words + 255) / 256, 256, 0, s>>>(bm, words, r.counts);
-  e = launch_scan(r.counts, words, r.offs, r.total, r.tiles, r.hdr_ctr, r.hist, r.err, s);
+  e = launch_scan(r.counts, words, r.offs, r.total, r.tiles, r.hdr_ctr, bin_limits(0, 0), r.hist,
+                  r.err, s);
   if (e == cudaSuccess) {
     k_emit_bits<<<(words + 255) / 256, 256, 0, s>>>(bm, words, r.offs, d_out);
     e = cudaGetLastError();

@@ -160,7 +160,7 @@ extern "C" int nspb_spgemm_rowblocked(const nspb_csr_in *A, const nspb_csr_in *B
       st = alloc_out(reinterpret_cast<void **>(&grpt), 4 * ((size_t)m + 1));
       if (!st) {
         e = launch_scan(len, (int)m, grpt, tot, reinterpret_cast<unsigned long long *>(ws + o_tiles),
-                        ctr, hist, errw, s);
+                        ctr, bin_limits(0, 0), hist, errw, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&g_nnz, tot, 8, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = NSPB_ERR_CUDA;

@@ -18,6 +18,21 @@
 
 namespace nspb {
 
+// ---- bin limits ------------------------------------------------------------------
+BinLimits bin_limits(int sym_fill_pct, int num_fill_pct) {
+  const int sf = sym_fill_pct <= 0 ? 75 : std::min(std::max(sym_fill_pct, 10), 90);
+  const int nf = num_fill_pct <= 0 ? 50 : std::min(std::max(num_fill_pct, 10), 50);
+  BinLimits l;
+  for (int b = 0; b < 16; ++b) {
+    // bin b's table has 32 << b slots
+    l.sym[b] = b < kSymLong ? std::max(1, (int)((32LL << b) * sf / 100)) : 0x7fffffff;
+    l.num[b] = b < kNumLong ? std::max(1, (int)((32LL << b) * nf / 100)) : 0x7fffffff;
+  }
+  return l;
+}
+int sym_bin_of(int ub, const BinLimits &l) { return sym_bin(ub, l); }
+int num_bin_of(int nz, const BinLimits &l) { return num_bin(nz, l); }
+
 // ---- B row order --------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     k_check_sorted(const int *__restrict__ rpt, const int *__restrict__ col,
@@ -70,7 +85,7 @@ constexpr int kRowinfoLong = 1024;
 
 template <int GA, bool MULTI>
 __global__ void __launch_bounds__(256)
-    k_rowinfo(const ProdTable<void> src, int n,
+    k_rowinfo(const ProdTable<void> src, int n, const BinLimits lim,
               int *__restrict__ row_nz, int64_t *__restrict__ row_ip,
               int *__restrict__ sym_counts,
               unsigned long long *__restrict__ total_ip, int *__restrict__ flags,
@@ -112,7 +127,7 @@ __global__ void __launch_bounds__(256)
       const int ub = (int)(ip < (long long)o.ncols ? ip : (long long)o.ncols);
       row_nz[row] = ub;
       if (row_ip) row_ip[row] = ip;
-      if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
+      if (ub > 0) atomicAdd(&hist[sym_bin(ub, lim)], 1);
       my_total += (unsigned long long)ip;
     }
   }
@@ -126,7 +141,7 @@ __global__ void __launch_bounds__(256)
 // The rows k_rowinfo listed: one block per row, the same outputs.
 template <bool MULTI>
 __global__ void __launch_bounds__(256)
-    k_rowinfo_long(const ProdTable<void> src, const int *__restrict__ long_list,
+    k_rowinfo_long(const ProdTable<void> src, const BinLimits lim, const int *__restrict__ long_list,
                    const int *__restrict__ long_count, int *__restrict__ row_nz,
                    int64_t *__restrict__ row_ip, int *__restrict__ sym_counts,
                    unsigned long long *__restrict__ total_ip, int *__restrict__ flags) {
@@ -160,7 +175,7 @@ __global__ void __launch_bounds__(256)
       const int ub = (int)(t < (long long)o.ncols ? t : (long long)o.ncols);
       row_nz[row] = ub;
       if (row_ip) row_ip[row] = t;
-      if (ub > 0) atomicAdd(&hist[sym_bin(ub)], 1);
+      if (ub > 0) atomicAdd(&hist[sym_bin(ub, lim)], 1);
       s_total += (unsigned long long)t;
     }
     __syncthreads();
@@ -171,7 +186,8 @@ __global__ void __launch_bounds__(256)
   if (threadIdx.x == 0 && s_total) atomicAdd(total_ip, s_total);
 }
 
-cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *row_nz,
+cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, const BinLimits &lim,
+                           int *row_nz,
                            int64_t *row_ip, int *sym_counts,
                            unsigned long long *total_ip, int *flags, int *long_list,
                            int *long_count, cudaStream_t s) {
@@ -182,9 +198,9 @@ cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *
                                           (int64_t)dev_info().sms * 8);
   const bool multi = t.prod_of_row != nullptr;
 #define NSPB_RI(GA)                                                                         \
-  (multi ? k_rowinfo<GA, true><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts, total_ip, \
+  (multi ? k_rowinfo<GA, true><<<grid, 256, 0, s>>>(t, n, lim, row_nz, row_ip, sym_counts, total_ip, \
                                                     flags, long_list, long_count)           \
-         : k_rowinfo<GA, false><<<grid, 256, 0, s>>>(t, n, row_nz, row_ip, sym_counts,       \
+         : k_rowinfo<GA, false><<<grid, 256, 0, s>>>(t, n, lim, row_nz, row_ip, sym_counts,       \
                                                      total_ip, flags, long_list, long_count))
   switch (ga) {
     case 32: NSPB_RI(32); break;
@@ -196,14 +212,14 @@ cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, int *
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !long_list) return e;
   auto klong = multi ? k_rowinfo_long<true> : k_rowinfo_long<false>;
-  klong<<<dev_info().sms * 4, 256, 0, s>>>(t, long_list, long_count, row_nz, row_ip, sym_counts,
+  klong<<<dev_info().sms * 4, 256, 0, s>>>(t, lim, long_list, long_count, row_nz, row_ip, sym_counts,
                                            total_ip, flags);
   return cudaGetLastError();
 }
 
 // ---- bin permutation ------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
-    k_perm(const int *__restrict__ key, int n, int kind, BinOffsets off,
+    k_perm(const int *__restrict__ key, int n, int kind, BinOffsets off, const BinLimits lim,
            int *__restrict__ cursor, int *__restrict__ perm) {
   __shared__ int hist[16];
   __shared__ int base[16];
@@ -214,7 +230,7 @@ __global__ void __launch_bounds__(1024)
   if (i < n) {
     const int k = kind == 0 ? key[i] : key[i + 1] - key[i];
     if (k > 0) {
-      b = kind == 0 ? sym_bin(k) : num_bin(k);
+      b = kind == 0 ? sym_bin(k, lim) : num_bin(k, lim);
       r = atomicAdd(&hist[b], 1);
     }
   }
@@ -225,10 +241,10 @@ __global__ void __launch_bounds__(1024)
   if (b >= 0) perm[base[b] + r] = i;
 }
 
-cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets,
+cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets, const BinLimits &lim,
                         int *cursor, int *perm, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_perm<<<(n + 1023) / 1024, 1024, 0, s>>>(key, n, kind, offsets, cursor, perm);
+  k_perm<<<(n + 1023) / 1024, 1024, 0, s>>>(key, n, kind, offsets, lim, cursor, perm);
   return cudaGetLastError();
 }
 
@@ -308,7 +324,8 @@ __device__ __forceinline__ void publish(unsigned long long *st, int t, long long
 __global__ void __launch_bounds__(kScanThreads)
     k_scan(const int *__restrict__ in, int n, int *__restrict__ out,
            long long *__restrict__ total, unsigned long long *tile_state,
-           int *tile_ctr, int *__restrict__ num_counts, int *__restrict__ err) {
+           int *tile_ctr, const BinLimits lim, int *__restrict__ num_counts,
+           int *__restrict__ err) {
   __shared__ int s_tile;
   __shared__ long long s_warp[kScanThreads / 32];
   __shared__ long long s_prefix;
@@ -332,7 +349,7 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
   for (int q = 0; q < kScanItems; ++q) {
     sum += v[q];
-    if (v[q] > 0) atomicAdd(&hist[num_bin(v[q])], 1);
+    if (v[q] > 0) atomicAdd(&hist[num_bin(v[q], lim)], 1);
   }
   // block scan of the per-thread sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -398,33 +415,35 @@ __global__ void __launch_bounds__(kScanThreads)
 }
 
 cudaError_t launch_scan(const int *row_nz, int n, int *crpt, long long *total,
-                        unsigned long long *tile_state, int *tile_ctr,
+                        unsigned long long *tile_state, int *tile_ctr, const BinLimits &lim,
                         int *num_counts, int *err, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   k_scan<<<scan_tiles(n), kScanThreads, 0, s>>>(row_nz, n, crpt, total, tile_state,
-                                                tile_ctr, num_counts, err);
+                                                tile_ctr, lim, num_counts, err);
   return cudaGetLastError();
 }
 
 // ---- numeric bins from an existing row pointer ---------------------------------
 __global__ void __launch_bounds__(1024)
-    k_num_hist(const int *__restrict__ crpt, int n, int *__restrict__ num_counts) {
+    k_num_hist(const int *__restrict__ crpt, int n, const BinLimits lim,
+               int *__restrict__ num_counts) {
   __shared__ int hist[kNumBins];
   if (threadIdx.x < kNumBins) hist[threadIdx.x] = 0;
   __syncthreads();
   const int i = blockIdx.x * 1024 + threadIdx.x;
   if (i < n) {
     const int k = crpt[i + 1] - crpt[i];
-    if (k > 0) atomicAdd(&hist[num_bin(k)], 1);
+    if (k > 0) atomicAdd(&hist[num_bin(k, lim)], 1);
   }
   __syncthreads();
   if (threadIdx.x < kNumBins && hist[threadIdx.x])
     atomicAdd(&num_counts[threadIdx.x], hist[threadIdx.x]);
 }
 
-cudaError_t launch_num_hist(const int *crpt, int n, int *num_counts, cudaStream_t s) {
+cudaError_t launch_num_hist(const int *crpt, int n, const BinLimits &lim, int *num_counts,
+                            cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_num_hist<<<(n + 1023) / 1024, 1024, 0, s>>>(crpt, n, num_counts);
+  k_num_hist<<<(n + 1023) / 1024, 1024, 0, s>>>(crpt, n, lim, num_counts);
   return cudaGetLastError();
 }
 

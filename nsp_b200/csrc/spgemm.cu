@@ -150,6 +150,7 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   t32 = ProdTable<float>{};
   t32.one = Operands<float>{A.rpt, A.col, A.val32, B.rpt, B.col, B.val32, B.ncols, B.nrows};
   info = ProdInfo{n, B.ncols, 1, B.nrows};
+  lim = bin_limits(opts.sym_fill_pct, opts.num_fill_pct);
   a_nnz = A.nnz;
   table = false;
   ops = nullptr;
@@ -290,7 +291,7 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     ++launches;
   }
   // perm is free until the bins are permuted: it holds the long-row list here
-  if ((e = launch_rowinfo(structure_of(t64), n, a_nnz, row_nz, nullptr, ctr->sym_counts,
+  if ((e = launch_rowinfo(structure_of(t64), n, a_nnz, lim, row_nz, nullptr, ctr->sym_counts,
                           &ctr->total_ip,
                           !opts.assume_sorted && same ? &ctr->flags : nullptr, perm,
                           &ctr->long_rows, s)) != cudaSuccess)
@@ -309,7 +310,7 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   const bool direct = nonempty == 1 && binned == n;
   mark(2);
   if (!direct && binned > 0) {
-    if ((e = launch_perm(row_nz, n, 0, off, ctr->cursor_sym, perm, s)) != cudaSuccess)
+    if ((e = launch_perm(row_nz, n, 0, off, lim, ctr->cursor_sym, perm, s)) != cudaSuccess)
       return cuda_fail(e);
     ++launches;
     if ((e = order_block_bins(row_nz, 0, h.sym_counts, kSymGroupBins, kSymBins, off)) != cudaSuccess)
@@ -325,7 +326,7 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     ++launches;
   }
   mark(3);
-  if ((e = launch_scan(row_nz, n, crpt, &ctr->total_nnz, tile_state, &ctr->tile_ctr,
+  if ((e = launch_scan(row_nz, n, crpt, &ctr->total_nnz, tile_state, &ctr->tile_ctr, lim,
                        ctr->num_counts, &ctr->err, s)) != cudaSuccess)
     return cuda_fail(e);
   ++launches;
@@ -347,7 +348,7 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
   const bool direct = nonempty == 1 && binned == n;
   mark(5);
   if (!direct) {
-    if ((e = launch_perm(crpt, n, 1, off, ctr->cursor_num, perm, s)) != cudaSuccess)
+    if ((e = launch_perm(crpt, n, 1, off, lim, ctr->cursor_num, perm, s)) != cudaSuccess)
       return cuda_fail(e);
     ++launches;
     if ((e = order_block_bins(crpt, 1, h.num_counts, kNumGroupBins, kNumBins, off)) != cudaSuccess)
@@ -400,7 +401,7 @@ int Call::prepare_numeric(const int *crpt) {
               : launch_check_sorted(B, &ctr->flags, s);
     if (e != cudaSuccess) return cuda_fail(e);
   }
-  if ((e = launch_num_hist(crpt, n, ctr->num_counts, s)) != cudaSuccess) return cuda_fail(e);
+  if ((e = launch_num_hist(crpt, n, lim, ctr->num_counts, s)) != cudaSuccess) return cuda_fail(e);
   launches += opts.assume_sorted ? 1 : 2;
   if ((st = fetch_counters())) return st;
   b_sorted = opts.assume_sorted || !(h.flags & B_UNSORTED);
@@ -654,7 +655,7 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip, 
     return NSPB_OK;
   }
   if ((st = call.alloc_scratch())) return st;
-  cudaError_t e = launch_rowinfo(structure_of(call.t64), call.n, call.a_nnz, call.row_nz,
+  cudaError_t e = launch_rowinfo(structure_of(call.t64), call.n, call.a_nnz, call.lim, call.row_nz,
                                  d_row_ip, call.ctr->sym_counts,
                                  &call.ctr->total_ip, nullptr, call.perm, &call.ctr->long_rows,
                                  call.s);

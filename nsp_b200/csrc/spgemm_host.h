@@ -47,6 +47,7 @@ struct Call {
   ProdTable<double> t64;
   ProdTable<float> t32;
   ProdInfo info;
+  BinLimits lim{};                  // bin thresholds (opts.sym_fill_pct, num_fill_pct)
   int64_t a_nnz = 0;                // entries of A over all products
   bool table = false;               // several products through a device table
   const Operands<void> *ops = nullptr;

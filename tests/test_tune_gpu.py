@@ -1,5 +1,6 @@
-"""The autotuner's knobs (threads per row, numeric table size) and the
-autotuner itself: every candidate is a valid, bit-exact configuration."""
+"""The autotuner's knobs (threads per row, kernel family, table size, symbolic
+and numeric bin thresholds) and the autotuner itself: every candidate is a
+valid, bit-exact configuration."""
 import numpy as np
 import pytest
 
@@ -25,14 +26,34 @@ def test_knobs_bitexact(cuda, lanes, shift):
     assert_bitwise(h.val, val)
 
 
+@pytest.mark.parametrize("row_kernel", [1, 2, 3])
+@pytest.mark.parametrize("fills", [(50, 25), (75, 37), (90, 50), (10, 10)])
+def test_bin_thresholds_bitexact(cuda, row_kernel, fills):
+    """Thresholds only move rows between bins whose kernels hold them."""
+    A = nb.gen.random(4000, 3000, 0, 40, seed=31)
+    B = nb.gen.random(3000, 2500, 1, 20, seed=32)
+    C, st = nb.spgemm(A.to_device(), B.to_device(), row_kernel=row_kernel,
+                      sym_fill_pct=fills[0], num_fill_pct=fills[1], return_stats=True)
+    rp, col, val = oracle.spgemm(A, B)
+    h = C.to_host()
+    assert_same_structure(h.rowptr, h.col, rp, col)
+    if sum(st["num_bins"][6:]) == 0:
+        assert_bitwise(h.val, val)
+    else:
+        from conftest import assert_close
+        assert_close(h.val, val, oracle.absbound(A, B, rp, col))
+
+
 def test_autotune_picks_a_measured_candidate(cuda):
     A = nb.gen.stencil(24, npts=27)
     dA = A.to_device()
     best, report = nb.autotune(dA, dA, reps=2)
-    assert len(report) == 6 and all(ms > 0 for _, _, ms in report)
-    fastest = min(report, key=lambda r: r[2])
-    assert (best["group_lanes"], best["table_shift"]) == fastest[:2]
-    C = nb.spgemm(dA, dA, group_lanes=best["group_lanes"], table_shift=best["table_shift"])
+    assert 6 <= len(report) <= 16 and all(ms > 0 for _, ms in report)
+    fastest = min(report, key=lambda r: r[1])
+    assert best == fastest[0]
+    C = nb.spgemm(dA, dA, group_lanes=best["group_lanes"], table_shift=best["table_shift"],
+                  row_kernel=best["row_kernel"], sym_fill_pct=best["sym_fill_pct"],
+                  num_fill_pct=best["num_fill_pct"])
     rp, col, val = oracle.spgemm(A, A)
     h = C.to_host()
     assert_same_structure(h.rowptr, h.col, rp, col)
