@@ -56,7 +56,7 @@ def parse():
                    help="stencil edge L (default 128; smaller grids for profiler captures)")
     p.add_argument("--no-forms", action="store_true",
                    help="skip the batched / fp32c / reference-kernel lines (profiler captures)")
-    p.add_argument("--form-steps", type=int, default=3,
+    p.add_argument("--form-steps", type=int, default=5,
                    help="timed steps of each form (after one warm-up step)")
     p.add_argument("--only-form", default=None, choices=["batched", "fp32c", "reference_gpu",
                                                           "powerlaw"],
@@ -90,7 +90,9 @@ def _timed(fn, steps, warmup):
 class _StepTimer:
     """Device time of single calls: synchronize, event, call, event, synchronize.
     Work released after a call (freeing its outputs) happens outside the
-    measured span, for every arm alike."""
+    measured span, for every arm alike. Returns the median over the steps:
+    device allocation inside the calls (cudaMalloc of C, as the reference's
+    entry point does) occasionally takes several ms."""
 
     def __init__(self):
         import torch
@@ -103,17 +105,17 @@ class _StepTimer:
             fn()
             if after:
                 after()
-        total = 0.0
+        times = []
         for _ in range(steps):
             torch.cuda.synchronize()
             self.e0.record()
             fn()
             self.e1.record()
             torch.cuda.synchronize()
-            total += self.e0.elapsed_time(self.e1)
+            times.append(self.e0.elapsed_time(self.e1))
             if after:
                 after()
-        return total / steps
+        return statistics.median(times)
 
 
 def form_batched(args, index):
@@ -141,8 +143,8 @@ def form_batched(args, index):
                       "products": len(pairs), "amg_products": n_amg,
                       "random_products": args.batch_count, "random_n": [1000, args.batch_nmax],
                       "random_degrees": [4, 32], "setup_s": round(setup_s, 1),
-                      "timing": "device time of each call, C allocated inside both arms, "
-                                "outputs freed outside the timed spans"}}
+                      "timing": "median device time of single calls, C allocated inside both "
+                                "arms, outputs freed outside the timed spans"}}
     clocks = Clocks(index)
     clocks.start()
     for name, sl in (("amg", slice(0, n_amg)), ("amg_plus_random", slice(0, len(pairs)))):
@@ -260,13 +262,15 @@ def form_reference_gpu(args, index, A, dA):
     lib = C.CDLL(oracle.REF_SO)
     lib.ref_nsp_time_device.restype = C.c_float
     lib.ref_nsp_time_device.argtypes = [C.c_int] * 3 + [C.c_void_p] * 3 + [C.c_int] + \
-        [C.c_void_p] * 3 + [C.c_int] * 3 + [C.POINTER(C.c_int)]
+        [C.c_void_p] * 3 + [C.c_int] * 3 + [C.POINTER(C.c_int), C.POINTER(C.c_float)]
     nnz = C.c_int(0)
     p = (dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr())
+    times = (C.c_float * args.form_steps)()
     clocks = Clocks(index)
     clocks.start()
-    ref_ms = lib.ref_nsp_time_device(A.nrows, A.ncols, A.ncols, *p, A.nnz, *p, A.nnz,
-                                     1, args.form_steps, C.byref(nnz))
+    lib.ref_nsp_time_device(A.nrows, A.ncols, A.ncols, *p, A.nnz, *p, A.nnz, 1, args.form_steps,
+                            C.byref(nnz), times)
+    ref_ms = statistics.median(list(times))  # the same statistic as this library's arm
     torch.cuda.synchronize()
     a = nb.sfcsr_of(dA)
     cs = []
@@ -291,6 +295,7 @@ def form_reference_gpu(args, index, A, dA):
                                        "nvcc -O3 -arch sm_100a -DDOUBLE"},
             "nspb_dropin": {"ms": ms, "gflops": flops / ms / 1e6},
             "speedup_nspb_vs_reference": ref_ms / ms, "steps": args.form_steps,
+            "statistic": "median of single calls (CUDA events, device synchronised around each)",
             "clocks": clk}
 
 

@@ -77,10 +77,11 @@ extern "C" void ref_free(void *p) { std::free(p); }
 // Milliseconds per call of nsp_spgemm_kernel_hash on device inputs (C is
 // allocated inside each call, as in the reference, and freed after it),
 // mean over `reps` calls after `warm` untimed calls, CUDA events on the
-// default stream. *nnz_out receives nnz(C).
+// default stream; times_out (may be NULL) receives every timed call's ms.
+// *nnz_out receives nnz(C).
 extern "C" float ref_nsp_time_device(int M, int K, int N, int *a_rpt, int *a_col, double *a_val,
                                      int annz, int *b_rpt, int *b_col, double *b_val, int bnnz,
-                                     int warm, int reps, int *nnz_out) {
+                                     int warm, int reps, int *nnz_out, float *times_out) {
   sfCSR a, b;
   std::memset(&a, 0, sizeof(a));
   std::memset(&b, 0, sizeof(b));
@@ -110,7 +111,10 @@ extern "C" float ref_nsp_time_device(int M, int K, int N, int *a_rpt, int *a_col
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    if (r >= warm) total += ms;
+    if (r >= warm) {
+      total += ms;
+      if (times_out) times_out[r - warm] = ms;
+    }
     *nnz_out = c.nnz;
     cudaFree(c.d_rpt);
     cudaFree(c.d_col);
