@@ -86,10 +86,17 @@ constexpr int kLongWords = kLongBits / 32;
 constexpr int kWideLog2T = 15;      // hash table of 2^15 ints: the same 128 KB
 constexpr int kWideHashMax = 3 << (kWideLog2T - 2);
 
-// 145 KB of shared memory a block: one block per SM, so the minimum of one
-// block lets ptxas use 64 registers a thread (it kept 32 without it)
-template <bool MULTI>
-__global__ void __launch_bounds__(kWideThreads, 1)
+// Blocks per SM given to __launch_bounds__: a bitmap of more than 2^19 bits
+// (64 KB) leaves room for one block per SM, which may then use 64 registers a
+// thread; a narrower one admits two, at 32 registers (the 250k power-law
+// product's first launch: 106 us at one block per SM, 72 us at two).
+constexpr int kWideTwoBlockSmem = 64 * 1024;
+__host__ __device__ constexpr int sym_wide_minb(int smem) {
+  return smem <= kWideTwoBlockSmem ? 2 : 1;
+}
+
+template <bool MULTI, int MINB>
+__global__ void __launch_bounds__(kWideThreads, MINB)
     k_sym_wide(const ProdTable<void> src, int b_sorted, const int *__restrict__ rows, int count,
                int *__restrict__ row_nz, int *__restrict__ err, int *__restrict__ ticket) {
   extern __shared__ __align__(16) unsigned bm[];
@@ -197,7 +204,9 @@ cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTab
   // the bitmap covers one window of B's columns at most; the hash table needs
   // the full 128 KB, which it only uses when B has more columns than a window
   const int smem = (int)std::min<long long>(kLongWords, ((long long)info.max_ncols + 31) >> 5) * 4;
-  auto kern = t.prod_of_row ? k_sym_wide<true> : k_sym_wide<false>;
+  const bool multi = t.prod_of_row != nullptr;
+  auto kern = sym_wide_minb(smem) == 2 ? (multi ? k_sym_wide<true, 2> : k_sym_wide<false, 2>)
+                                       : (multi ? k_sym_wide<true, 1> : k_sym_wide<false, 1>);
   const int grid = persistent_grid((const void *)kern, kWideThreads, smem, count, 1);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, kWideThreads, smem, s>>>(t, b_sorted ? 1 : 0, rows, count, row_nz, err, ticket);
