@@ -200,12 +200,14 @@ int nspb_intprod(const nspb_csr_in *A, const nspb_csr_in *B, int64_t *d_row_ip,
                  int64_t *total, void *stream);
 
 /* ---- batched products ------------------------------------------------------ */
-/* `count` independent products C[i] = A[i]·B[i] run as one block-diagonal
- * product: one launch per phase and bin over the rows of all products (a
- * single bin-sorted work queue across products), two host synchronisations
- * per group of products (groups keep nnz(C) below int32). C[i] are views into
- * per-group allocations; their base pointers are written to owners (room for
- * 3*count) and *n_owners; release them with nspb_free.                       */
+/* `count` independent products C[i] = A[i]·B[i] through one pipeline: the
+ * rows of all products form one work list, read through per-product operand
+ * descriptors and a row-to-product map (no copies of A or B), with one launch
+ * per phase and bin. Products are grouped so that each group's nnz(C) stays
+ * below int32; a group reads back to the host the bin counts, nnz(C), the
+ * error word (when checked) and C's per-product offsets. C[i] are views into one allocation
+ * per group (values, columns, row pointers); their base pointers are written
+ * to owners (room for 3*count) and *n_owners; release them with nspb_free.  */
 int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_csr_in *B,
                         nspb_csr_out *C, const nspb_opts *opts,
                         nspb_stats *stats, void **owners, int32_t *n_owners);

@@ -196,9 +196,27 @@ static void table_views(const TableHost &h, const nspb_csr_in *A, const nspb_csr
   }
 }
 
+// Statistics of a group of products added into those of the call.
+static void add_stats(nspb_stats &t, const nspb_stats &g) {
+  t.intprod += g.intprod;
+  t.nnz += g.nnz;
+  t.launches += g.launches;
+  t.rows_redone += g.rows_redone;
+  t.max_row_err = std::max(t.max_row_err, g.max_row_err);
+  for (int b = 0; b < 16; ++b) {
+    t.sym_bins[b] += g.sym_bins[b];
+    t.num_bins[b] += g.num_bins[b];
+  }
+  t.b_sorted = g.b_sorted;
+  t.ms_rowinfo += g.ms_rowinfo;
+  t.ms_symbolic += g.ms_symbolic;
+  t.ms_scan += g.ms_scan;
+  t.ms_numeric += g.ms_numeric;
+}
+
 // One group of products through one pipeline. On success C[p] are views into
-// two allocations (C col/val) plus the row-pointer block; the three base
-// pointers are appended to owners.
+// one allocation (values, columns, row pointers), whose base pointer is
+// appended to owners.
 static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, nspb_csr_out *C,
                          const nspb_opts &o, nspb_stats *stats, void **owners, int *n_owners) {
   cudaStream_t s = static_cast<cudaStream_t>(o.stream);
@@ -223,12 +241,22 @@ static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, 
   int64_t nnz = 0;
   int *ccol = nullptr, *rp_all = nullptr;
   double *cval = nullptr;
+  // C's values, columns and row pointers in one allocation, in that order
+  // (each part starts on a 16-byte boundary)
+  char *cbase = nullptr;
   st = call.symbolic(crp, &nnz);
-  if (!st) st = alloc_out(reinterpret_cast<void **>(&ccol), (size_t)nnz * 4);
-  if (!st) st = alloc_out(reinterpret_cast<void **>(&cval), (size_t)nnz * 8);
+  if (!st) {
+    const size_t o_col = ((size_t)nnz * 8 + 15) & ~(size_t)15;
+    const size_t o_rp = (o_col + (size_t)nnz * 4 + 15) & ~(size_t)15;
+    st = alloc_out(reinterpret_cast<void **>(&cbase), o_rp + 4 * (size_t)(h.rows + count));
+    if (!st) {
+      cval = reinterpret_cast<double *>(cbase);
+      ccol = reinterpret_cast<int *>(cbase + o_col);
+      rp_all = reinterpret_cast<int *>(cbase + o_rp);
+    }
+  }
   if (!st) st = call.numeric(crp, ccol, cval);
   if (!st) st = call.finish(stats);
-  if (!st) st = alloc_out(reinterpret_cast<void **>(&rp_all), 4 * (size_t)(h.rows + count));
   std::vector<int> starts;
   if (!st) {
     table_split(h, ws, rp_all, s);
@@ -243,15 +271,11 @@ static int batched_group(int count, const nspb_csr_in *A, const nspb_csr_in *B, 
   cudaStreamSynchronize(s);
   scratch_free(ws, s);
   if (st) {
-    if (rp_all) cudaFree(rp_all);
-    if (ccol) cudaFree(ccol);
-    if (cval) cudaFree(cval);
+    if (cbase) cudaFree(cbase);
     return st;
   }
   table_views(h, A, B, starts, rp_all, ccol, cval, C);
-  owners[(*n_owners)++] = rp_all;
-  owners[(*n_owners)++] = ccol;
-  owners[(*n_owners)++] = cval;
+  owners[(*n_owners)++] = cbase;
   return NSPB_OK;
 }
 
@@ -263,7 +287,10 @@ constexpr double kGroupIntprod = 1.2e9;
 static int batched_range(int first, int count, const nspb_csr_in *A, const nspb_csr_in *B,
                          nspb_csr_out *C, const nspb_opts &o, nspb_stats *stats, void **owners,
                          int *n_owners) {
-  int st = batched_group(count, A + first, B + first, C + first, o, stats, owners, n_owners);
+  nspb_stats gs;
+  std::memset(&gs, 0, sizeof(gs));
+  int st = batched_group(count, A + first, B + first, C + first, o, &gs, owners, n_owners);
+  if (!st) add_stats(*stats, gs);
   if (st == NSPB_ERR_OVERFLOW && count > 1) {
     const int h = count / 2;
     st = batched_range(first, h, A, B, C, o, stats, owners, n_owners);
@@ -307,16 +334,7 @@ extern "C" int nspb_spgemm_batched(int count, const nspb_csr_in *A, const nspb_c
       *n_owners = 0;
       return st;
     }
-    total.intprod += gs.intprod;
-    total.nnz += gs.nnz;
-    total.launches += gs.launches;
-    total.rows_redone += gs.rows_redone;
-    total.max_row_err = std::max(total.max_row_err, gs.max_row_err);
-    for (int b = 0; b < 16; ++b) {
-      total.sym_bins[b] += gs.sym_bins[b];
-      total.num_bins[b] += gs.num_bins[b];
-    }
-    total.b_sorted = gs.b_sorted;
+    add_stats(total, gs);
     first = last;
   }
   *n_owners = n_own;
@@ -395,18 +413,6 @@ int group_numeric(PlanGroup &G, cudaStream_t s) {
   return G.call.numeric(crp, G.ccol, G.cval);
 }
 
-void add_stats(nspb_stats &t, const nspb_stats &g) {
-  t.intprod += g.intprod;
-  t.nnz += g.nnz;
-  t.launches += g.launches;
-  t.rows_redone += g.rows_redone;
-  t.max_row_err = std::max(t.max_row_err, g.max_row_err);
-  for (int b = 0; b < 16; ++b) {
-    t.sym_bins[b] += g.sym_bins[b];
-    t.num_bins[b] += g.num_bins[b];
-  }
-  t.b_sorted = g.b_sorted;
-}
 
 // Symbolic phase, C's arrays and one checked numeric pass of the products
 // [0, count); the C views are filled.

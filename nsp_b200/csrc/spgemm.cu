@@ -103,13 +103,18 @@ HostStage *host_stage() {
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-// Lanes per row group from the mean length of the B rows the products read.
-// Measured on B200: 32 lanes win from a mean of 8 entries up (random, AMG and
-// stencil products); 8 lanes below that when A has enough rows to fill the GPU
-// with the smaller groups (7-point Laplacian 128^3, mean 6.9: 2.7 ms with 8
-// lanes, 4.7 ms with 32).
-static int pick_lanes(double mean_b_row, int a_rows) {
-  return (mean_b_row < 7.5 && a_rows >= 65536) ? 8 : 32;
+// Lanes per row group from the mean length of the B rows the products read
+// and of A's rows. Measured on B200 (one call, C allocated inside): 32 lanes
+// win from a mean B row of 8 entries up (random, AMG and stencil products).
+// Below that, when A has enough rows to fill the GPU with smaller groups, 8
+// lanes win on short A rows (7-point Laplacian 128^3, 7 entries a row: 3.38 ms
+// with 8 lanes, 3.87 with 16, 5.11 with 32) and 16 on longer ones, which 8
+// lanes stage in too many rounds (27-point stencil 96^3 times its smoothed
+// aggregation prolongator, 27 A entries a row and B rows of 4.5: 3.53 ms with
+// 16 lanes, 4.61 with 8, 4.00 with 32).
+static int pick_lanes(double mean_b_row, double mean_a_row, int a_rows) {
+  if (mean_b_row < 7.5 && a_rows >= 65536) return mean_a_row <= 8.0 ? 8 : 16;
+  return 32;
 }
 
 // ---- a call --------------------------------------------------------------------
@@ -163,7 +168,7 @@ int Call::init(const nspb_csr_in *a, const nspb_csr_in *b, const nspb_opts *o) {
   } else {
     // until the intermediate products are counted (symbolic): B's mean row
     const double avg = B.nrows > 0 ? (double)B.nnz / (double)B.nrows : 0.0;
-    lanes = pick_lanes(avg, A.nrows);
+    lanes = pick_lanes(avg, A.nrows > 0 ? (double)A.nnz / (double)A.nrows : 0.0, A.nrows);
   }
   return NSPB_OK;
 }
@@ -304,7 +309,7 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
   // the mean length of the B rows actually read, weighted by how often A reads
   // them: a block-diagonal batch mixes products whose B rows differ
   if (!(opts.group_lanes == 8 || opts.group_lanes == 16 || opts.group_lanes == 32) && a_nnz > 0)
-    lanes = pick_lanes((double)intprod / (double)a_nnz, n);
+    lanes = pick_lanes((double)intprod / (double)a_nnz, (double)a_nnz / (double)n, n);
   int nonempty = 0, binned = 0;
   BinOffsets off = offsets_of(h.sym_counts, kSymBins, &nonempty, &binned);
   const bool direct = nonempty == 1 && binned == n;
