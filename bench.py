@@ -37,9 +37,10 @@ sys.path.insert(0, ROOT)
 
 L = 128
 SEED = 20261203
-# the row-group kernels the default call runs (dominant launches of the stencil product)
-NUM_KERNEL = "k_num_rg"
-SYM_KERNEL = "k_sym_group"
+# the row-group kernels the default call runs (dominant launches of the stencil
+# product): from entry maps when the call recorded them, else the staged walk
+NUM_KERNEL = {True: "k_num_map", False: "k_num_rg"}
+SYM_KERNEL = {True: "k_sym_map", False: "k_sym_group"}
 METRIC = "SpGEMM GFLOP/s, C=A*A, 27-point stencil 128^3, fp64"
 WORKLOAD = "stencil27_128^3_AxA_fp64"
 
@@ -628,11 +629,11 @@ def main():
     if dominant == "numeric":
         kbytes = alg_bytes(Ah, Bh, nnz_c)
         kms = phase["ms_numeric"]
-        kname = NUM_KERNEL
+        kname = NUM_KERNEL[bool(stats.entry_map)]
     else:
         kbytes = 4 * (Ah.nrows + 1) + 4 * Ah.nnz + 4 * (Bh.nrows + 1) + 4 * Bh.nnz + 4 * Ah.nrows
         kms = phase["ms_symbolic"]
-        kname = SYM_KERNEL
+        kname = SYM_KERNEL[bool(stats.entry_map)]
     achieved = kbytes / (kms * 1e-3) / 1e9 if kms > 0 else 0.0
     traffic = profiled_traffic(kname)
 

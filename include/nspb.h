@@ -121,7 +121,14 @@ typedef struct {
                             of C), else hash tables with an in-table sort;
                             1 = always the hash-sort kernels; 2 = always the
                             staged walk (tables of 4x the bin's row limit);
-                            3 = staged walk with tables of 2x              */
+                            3 = staged walk with tables of 2x; 7 = entry
+                            maps: the symbolic pass records each product's
+                            entry index in its row and the numeric rows of
+                            <= 256 entries add at that index with no hash
+                            table (0 takes maps when the B rows read fill
+                            3/4 of the row groups' lanes on average; maps
+                            need fp64, one-call products, sorted B rows, no
+                            row of more than 3072 products, < 2^24 columns) */
   int32_t sym_fill_pct;  /* symbolic bin thresholds: a row goes to the bin
                             whose table (32 << b slots) it fills to at most
                             this percentage at its upper bound of distinct
@@ -146,7 +153,10 @@ typedef struct {
   float ms_symbolic;     /* opts.timing: permutation + symbolic kernels      */
   float ms_scan;         /* opts.timing: row_ptr scan                        */
   float ms_numeric;      /* opts.timing: permutation + numeric kernels       */
-  float _pad;
+  int32_t entry_map;     /* 1 if the symbolic phase recorded entry maps and
+                            the numeric row-group bins of <= 256 entries ran
+                            from them (opts.row_kernel 0 or 7); batched
+                            calls and plans: the number of such groups     */
 } nspb_stats;
 
 /* ---- library ------------------------------------------------------------ */

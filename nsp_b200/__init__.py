@@ -67,7 +67,8 @@ def make_opts(precision=PREC_FP64, assume_sorted=False, check_errors=True, group
 def stats_dict(s: Stats) -> dict:
     return {"intprod": s.intprod, "nnz": s.nnz, "sym_bins": list(s.sym_bins)[:12],
             "num_bins": list(s.num_bins)[:10], "rows_redone": s.rows_redone,
-            "b_sorted": s.b_sorted, "max_row_err": s.max_row_err, "launches": s.launches}
+            "b_sorted": s.b_sorted, "max_row_err": s.max_row_err, "launches": s.launches,
+            "entry_map": s.entry_map}
 
 
 def spgemm(A: DeviceCSR, B: DeviceCSR, precision: str = "fp64", out: DeviceCSR | None = None,

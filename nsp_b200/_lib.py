@@ -65,7 +65,7 @@ class Stats(C.Structure):
                 ("rows_redone", C.c_int32), ("b_sorted", C.c_int32),
                 ("max_row_err", C.c_double), ("launches", C.c_int32),
                 ("ms_rowinfo", C.c_float), ("ms_symbolic", C.c_float),
-                ("ms_scan", C.c_float), ("ms_numeric", C.c_float), ("_pad", C.c_float)]
+                ("ms_scan", C.c_float), ("ms_numeric", C.c_float), ("entry_map", C.c_int32)]
 
 
 class TuneEntry(C.Structure):

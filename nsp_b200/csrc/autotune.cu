@@ -7,11 +7,11 @@
 // at every candidate value with the best values found so far for the others,
 // and kept at its fastest. Candidates, in search order:
 //   group_lanes     8, 16, 32
-//   row_kernel      1 (hash tables, in-table sort), 2 (staged walk)
+//   row_kernel      1 (hash tables, in-table sort), 2 (staged walk), 7 (entry maps)
 //   table size      hash-sort: num_table_shift 0, 1; staged: row_kernel 2, 3
 //   sym_fill_pct    50, 75, 90
 //   num_fill_pct    25, 37, 50
-// 12 timed candidates at most (the default of each knob is timed once).
+// 13 timed candidates at most (the default of each knob is timed once).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -123,12 +123,14 @@ extern "C" int nspb_autotune(const nspb_csr_in *A, const nspb_csr_in *B, const n
   Knobs k{32, 0, 1, 75, 50};
   float k_ms = 1e30f;
   if (!st) st = t.time(k, &k_ms);
-  static const int lanes[] = {8, 16, 32}, kinds[] = {1, 2}, fills_s[] = {50, 75, 90},
+  static const int lanes[] = {8, 16, 32}, kinds[] = {1, 2, 7}, fills_s[] = {50, 75, 90},
                    fills_n[] = {25, 37, 50};
   if (!st) st = t.sweep(k, k_ms, lanes, 3, [](Knobs &x, int v) { x.lanes = v; });
-  if (!st) st = t.sweep(k, k_ms, kinds, 2, [](Knobs &x, int v) { x.rk = v; });
+  if (!st) st = t.sweep(k, k_ms, kinds, 3, [](Knobs &x, int v) { x.rk = v; });
   if (!st) {
-    if (k.rk == 1) {
+    if (k.rk == 7) {
+      // entry maps have no table size
+    } else if (k.rk == 1) {
       static const int shifts[] = {0, 1};
       st = t.sweep(k, k_ms, shifts, 2, [](Knobs &x, int v) { x.tshift = v; });
     } else {

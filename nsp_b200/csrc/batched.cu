@@ -208,6 +208,7 @@ static void add_stats(nspb_stats &t, const nspb_stats &g) {
     t.num_bins[b] += g.num_bins[b];
   }
   t.b_sorted = g.b_sorted;
+  t.entry_map += g.entry_map;  // groups whose numeric phase ran from entry maps
   t.ms_rowinfo += g.ms_rowinfo;
   t.ms_symbolic += g.ms_symbolic;
   t.ms_scan += g.ms_scan;
@@ -358,6 +359,7 @@ struct PlanGroup {
   double *cval = nullptr;
   long long nnz = 0;
   ~PlanGroup() {
+    call.s = nullptr;  // the capture stream is gone: the call's pool blocks go back on the legacy stream
     for (void *p : {(void *)ws_tab, (void *)ws_call, (void *)crp, (void *)rp_all, (void *)ccol,
                     (void *)cval})
       if (p) cudaFree(p);

@@ -95,6 +95,16 @@ __device__ __forceinline__ int ld_stream(const int *p) {
   asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
   return v;
 }
+__device__ __forceinline__ unsigned ld_stream(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ unsigned ld_stream(const unsigned char *p) {
+  unsigned short v;
+  asm volatile("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
+}
 __device__ __forceinline__ double ld_stream(const double *p) {
   double v;
   asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
@@ -391,6 +401,16 @@ __device__ __forceinline__ int next_row(int *ticket, int count, int *s_slot) {
   __syncthreads();
   const int r = *s_slot;
   return r < count ? r : count;
+}
+
+// Entry-map layout (k_sym_map writes, k_num_map reads): four consecutive
+// steps of a chunk form a quad, stored as one 4-byte word per lane, when each
+// of their B rows fits the group of G lanes and they hold at least 3G
+// products (so the words waste at most a quarter of their bytes).
+template <int G>
+__device__ __forceinline__ bool map_quad(const int (&len)[4]) {
+  return len[0] <= G && len[1] <= G && len[2] <= G && len[3] <= G &&
+         len[0] + len[1] + len[2] + len[3] >= 3 * G;
 }
 
 // Monotone bucket map of a key in [lo, lo+range) onto [0, nb): used to sort

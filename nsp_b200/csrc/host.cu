@@ -245,6 +245,7 @@ extern "C" int nspb_spgemm_host(const nspb_csr_in *hA, const nspb_csr_in *hB, in
   bool b_sorted = true;
   {
     Call sym;
+    sym.allow_map = false;  // the row blocks' numeric steps run in their own calls
     if (!(st = sym.init(&dA, &dB, &o))) st = sym.symbolic(crpt, &nnz);
     b_sorted = sym.b_sorted;
   }

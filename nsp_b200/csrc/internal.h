@@ -13,6 +13,7 @@ struct DevInfo {
   int device = -1;
   int sms = 0;
   int smem_optin = 0;  // max dynamic shared memory per block (opt-in)
+  size_t total_mem = 0;  // device memory in bytes
 };
 // Properties of the current device (cached per device).
 const DevInfo &dev_info();
@@ -94,8 +95,28 @@ BinLimits bin_limits(int sym_fill_pct, int num_fill_pct);
 int sym_bin_of(int ub, const BinLimits &l);
 int num_bin_of(int nz, const BinLimits &l);
 
-// Flag bits written by launch_check_sorted.
-enum : int { B_UNSORTED = 1 };
+// Flag bits: B_UNSORTED written by launch_check_sorted (and k_rowinfo);
+// MAP_OVERFLOW by the map-recording symbolic kernels when a row has more
+// intermediate products than its map stride (the call then drops the map).
+enum : int { B_UNSORTED = 1, MAP_OVERFLOW = 2 };
+
+// ---- entry maps ------------------------------------------------------------------
+// The symbolic row-group kernels can record, for every intermediate product
+// of a row, the index of its column among the row's distinct columns in
+// order of first appearance (one byte; rows of more than 256 entries are not
+// served). map_off[row] gives the row's map in 16-byte units from the map
+// base, or kNoMap.
+constexpr unsigned kNoMap = 0xffffffffu;
+constexpr unsigned kMapEmpty = 0xffffffffu;   // empty slot of the map tables
+constexpr int kMapMaxCols = (1 << 24) - 2;    // column offsets take 24 bits
+constexpr int kMapNumBins = 5;                // numeric bins served: <= 256 entries
+struct MapArgs {
+  unsigned char *map = nullptr;  // the call's map
+  long long bin_off = 0;         // bytes from map to this bin's first row
+  int stride = 0;                // bytes per row (a multiple of 16)
+  unsigned *map_off = nullptr;   // per global row
+  int *flags = nullptr;          // MAP_OVERFLOW
+};
 
 // fp32 input modes (compensated pairs, or fp64 accumulation of exact products).
 inline bool fp32_inputs(int precision) {
@@ -164,6 +185,13 @@ cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTab
                                 const ProdInfo &info, const int *rows, int count,
                                 int *row_nz, int *err, int *ticket, cudaStream_t s);
 
+// Row-group symbolic bin (bin < kSymGroupBins) that also writes the entry
+// map of each row (B rows strictly increasing; every product's B has at
+// most kMapMaxCols columns).
+cudaError_t launch_symbolic_map(int bin, int lanes, const ProdTable<void> &t, const int *rows,
+                                int count, int *row_nz, int *err, const MapArgs &m,
+                                cudaStream_t s);
+
 // ---- numeric.cu -----------------------------------------------------------------
 // owned: B rows hold no duplicate columns (deterministic plain accumulation).
 // tshift: the row-group bins use tables 2^tshift times their default size.
@@ -201,4 +229,12 @@ cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth,
                                    double *cval, const int *rows, int count, int nmax,
                                    int *redo, int *max_deg, int *err, cudaStream_t s);
 
+// ---- rowmap.cu ------------------------------------------------------------------
+// Numeric row-group bin (bin < kMapNumBins) from the entry maps of a
+// map-recording symbolic phase: no hash table; fp64, B rows strictly
+// increasing.
+cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
+                               const unsigned char *map, const unsigned *map_off,
+                               const int *crpt, int *ccol, double *cval, const int *rows,
+                               int count, int *err, cudaStream_t s);
 }  // namespace nspb

@@ -96,6 +96,7 @@ extern "C" int nspb_spgemm_noalloc(const nspb_csr_in *A, const nspb_csr_in *B,
   if (o.precision != NSPB_PREC_FP64) return NSPB_ERR_UNSUPPORTED;
   o.timing = 0;  // events are resources this entry does not create
   Call call;
+  call.allow_map = false;  // the entry maps would need memory of their own
   int st = call.init(A, B, &o);
   if (st) return st;
   if (call.scratch_bytes() > kNoAllocScratch) {  // more rows than the array serves

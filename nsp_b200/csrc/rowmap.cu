@@ -1,0 +1,323 @@
+// Numeric kernels of the row-group bins that read the entry maps recorded by
+// the symbolic phase (k_sym_map in symbolic.cu): rows of at most 256 entries,
+// B rows strictly increasing, fp64.
+//
+// Reference counterparts (amavliut/nsp, nsp/src/nsp.cu):
+//   nsp_calculate_value_col_bin_mpwarp / _each_warp :1307-1494 (shared-memory
+//   hash of (column, value) slots with atomic adds, then an O(nnz^2) rank sort)
+//
+// The symbolic phase has already probed a hash table for every intermediate
+// product to count the row's distinct columns; k_sym_map also records, per
+// product, the index of its column among the row's distinct columns in order
+// of first appearance. The numeric walk here then adds a*b into a dense
+// value array at that index: no hash table, no probe loop, no CAS, and no
+// compaction of a table before the sort. The bound is still the shared-memory
+// data pipe (value updates and the sort).
+#include "common.cuh"
+#include "internal.h"
+#include "launch_util.h"
+
+namespace nspb {
+
+// Sort bucket of r in [0, span) for nb buckets: high 32 bits of r * mul,
+// mul ~ nb * 2^32 / span (single-precision estimate), clamped to nb - 1.
+// Monotone in r, so keys in lower buckets are smaller.
+__device__ __forceinline__ unsigned map_bucket_mul(unsigned span, int nb) {
+  const float m = (float)nb * 4294967296.0f / (float)(span ? span : 1u);
+  return m >= 4294967040.0f ? 0xffffffffu : (unsigned)m;
+}
+__device__ __forceinline__ int map_bucket(unsigned r, unsigned mul, int nb) {
+  const int b = (int)__umulhi(r, mul);
+  return b < nb - 1 ? b : nb - 1;
+}
+
+// ---- numeric from entry maps ---------------------------------------------------
+// Rows of at most 256 entries whose symbolic pass recorded the entry map
+// (k_sym_map): every intermediate product carries the index of its column
+// among the row's distinct columns in order of first appearance, so the walk
+// adds a*b into vals[index] with no hash table and no probe. The walk order
+// here equals the symbolic walk's (A entries in order, each B row's entries
+// in order, chunks of G A entries), so the new columns of a step are exactly
+// the indices at or past the count before the step; their lanes record the
+// column. Quads of the map (map_quad) give each lane one 4-byte word for four
+// steps; elsewhere each product has one byte. The row
+// is then sorted by the bucket counting sort over [first, last column] and
+// stored at its ranks.
+// Per group: vals[H] fp64, keys[H], info[H] (index inside the bucket), cnt[H],
+// bkey[H] (keys in bucket order), stage[G].
+template <int G, int LOG2H>
+struct NumMapCfg {
+  static constexpr int H = 1 << LOG2H;
+  static constexpr int BYTES = (H * 8 + H * 16 + G * 16 + 15) & ~15;
+  static constexpr int kBySmem = (56 * 1024) / BYTES > 0 ? (56 * 1024) / BYTES : 1;
+  static constexpr int GPC = kBySmem < 256 / G ? kBySmem : 256 / G;
+  static constexpr int THREADS = GPC * G;
+  static constexpr int SMEM = GPC * BYTES;
+};
+
+template <int G, int LOG2H, bool MULTI>
+__global__ void __launch_bounds__(256)
+    k_num_map(const ProdTable<double> src, const unsigned char *__restrict__ map,
+              const unsigned *__restrict__ map_off, const int *__restrict__ crpt,
+              int *__restrict__ ccol, double *__restrict__ cval, const int *__restrict__ rows,
+              int count, int *__restrict__ err) {
+  using C = NumMapCfg<G, LOG2H>;
+  constexpr int H = C::H;
+  extern __shared__ __align__(16) unsigned char smem_nmap[];
+  auto tile = cg::tiled_partition<G>(cg::this_thread_block());
+  const int g = threadIdx.x / G;
+  const int lane = tile.thread_rank();
+  unsigned char *gb = smem_nmap + (size_t)g * C::BYTES;
+  double *vals = reinterpret_cast<double *>(gb);
+  int *keys = reinterpret_cast<int *>(gb + (size_t)H * 8);
+  int *info = keys + H;
+  int *cnt = info + H;
+  int *bkey = cnt + H;
+  int4 *stage = reinterpret_cast<int4 *>(bkey + H);
+  int4 *c4 = reinterpret_cast<int4 *>(cnt);
+  for (int s = lane; s < H / 4; s += G) c4[s] = make_int4(0, 0, 0, 0);
+  tile.sync();
+
+  for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
+    const int row = rows ? rows[r] : r;
+    const int c0 = crpt[row];
+    const int n = crpt[row + 1] - c0;
+    if (n == 0) continue;  // no products (the group touched no shared state)
+    const unsigned mo = map_off[row];
+    if (n > H || mo == kNoMap) {
+      if (lane == 0) atomicOr(err, ERR_COUNT);
+      continue;
+    }
+    const unsigned char *mp = map + (size_t)mo * 16;
+    Operands<double> op;
+    const int lr = prod_row<MULTI>(src, row, op);
+    const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
+    const double *aval = op.aval, *bval = op.bval;
+    const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
+    int mn = 0x7fffffff, mx = -1;
+    int nk = 0;   // distinct columns before the current step (uniform)
+    int pos = 0;  // products walked so far (uniform)
+    // one product: index ix, column c, value p. The new columns of a step
+    // hold the indices from nk on; nf counts them within the step.
+    bool bad = false;
+    int nf = 0;
+    auto add = [&](bool has, unsigned ix, int c, double p) {
+      if (has && ix >= (unsigned)n) {  // not an index of this row: corrupt map
+        bad = true;
+        has = false;
+      }
+      const bool fresh = has && (int)ix >= nk;
+      nf += __popc(tile.ballot(fresh));
+      if (fresh) {
+        keys[ix] = c;
+        vals[ix] = __dadd_rn(0.0, p);
+      } else if (has) {
+        vals[ix] = __dadd_rn(vals[ix], p);
+      }
+    };
+    for (int ab = a0; ab < a1; ab += G) {
+      const int j = ab + lane;
+      if (j < a1) {
+        const int k = ld_stream(acol + j);
+        const double av = ldv_stream(aval + j);
+        const int bs = __ldg(brpt + k), be = __ldg(brpt + k + 1);
+        if (be > bs) {
+          mn = min(mn, __ldg(bcol + bs));
+          mx = max(mx, __ldg(bcol + be - 1));
+        }
+        stage[lane] = make_int4(bs, be, __double2loint(av), __double2hiint(av));
+      }
+      tile.sync();
+      const int na = min(G, a1 - ab);
+      int t = 0;
+      {
+        // quads of the map (map_quad): four B rows a round, one 4-byte word
+        // of indices per lane; indices, columns and values loaded before the
+        // first add; the adds still go step by step in A-row order
+        constexpr int D = 4;
+        for (; t + D <= na; t += D) {
+          int4 q[D];
+          int len[D];
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            q[i] = stage[t + i];
+            len[i] = q[i].y - q[i].x;
+          }
+          if (!map_quad<G>(len)) break;  // the step loop below takes the rest
+          const int pa = (pos + 3) & ~3;
+          const unsigned w = ld_stream(reinterpret_cast<const unsigned *>(mp + pa) + lane);
+          pos = pa + 4 * G;
+          unsigned ix[D];
+          int kc[D];
+          double b[D];
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            const int e = q[i].x + lane;
+            const bool has = lane < len[i];
+            ix[i] = (w >> (8 * i)) & 0xffu;
+            kc[i] = has ? __ldg(bcol + e) : 0;
+            b[i] = has ? __ldg(bval + e) : 0.0;
+          }
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            add(lane < len[i], ix[i], kc[i], __dmul_rn(__hiloint2double(q[i].w, q[i].z), b[i]));
+            nk += nf;
+            nf = 0;
+            tile.sync();  // the next step may hit the same entries
+          }
+        }
+      }
+      // the rest of the chunk: one map byte per product; four B rows loaded
+      // ahead while they fit the group
+      for (; t + 4 <= na; t += 4) {
+        int4 q[4];
+        bool fit = true;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          q[i] = stage[t + i];
+          fit &= q[i].y - q[i].x <= G;
+        }
+        if (!fit) break;
+        unsigned ix[4];
+        int kc[4];
+        double b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int e = q[i].x + lane;
+          const bool has = e < q[i].y;
+          ix[i] = has ? ld_stream(mp + pos + lane) : 0u;
+          kc[i] = has ? __ldg(bcol + e) : 0;
+          b[i] = has ? __ldg(bval + e) : 0.0;
+          pos += q[i].y - q[i].x;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          add(q[i].x + lane < q[i].y, ix[i], kc[i],
+              __dmul_rn(__hiloint2double(q[i].w, q[i].z), b[i]));
+          nk += nf;
+          nf = 0;
+          tile.sync();  // the next step may hit the same entries
+        }
+      }
+      for (; t < na; ++t) {
+        const int4 q = stage[t];
+        const double a = __hiloint2double(q.w, q.z);
+        for (int eb = q.x; eb < q.y; eb += G) {  // uniform trip count across the group
+          const int e = eb + lane;
+          const bool has = e < q.y;
+          const unsigned ix = has ? ld_stream(mp + pos + (e - q.x)) : 0u;
+          const int kc = has ? __ldg(bcol + e) : 0;
+          const double bv = has ? __ldg(bval + e) : 0.0;
+          add(has, ix, kc, __dmul_rn(a, bv));
+        }
+        pos += q.y - q.x;
+        nk += nf;
+        nf = 0;
+        tile.sync();  // the next step may hit the same entries
+      }
+    }
+    mn = cg::reduce(tile, mn, cg::less<int>());
+    mx = cg::reduce(tile, mx, cg::greater<int>());
+    if (tile.any(bad) || nk != n) {  // map and row pointer disagree: skip the row
+      if (lane == 0) atomicOr(err, ERR_COUNT);
+      tile.sync();
+      continue;
+    }
+    const unsigned mul = map_bucket_mul((unsigned)mx - (unsigned)mn + 1u, H);
+    // -- bucket counts, each key's place inside its bucket
+    for (int q = lane; q < n; q += G)
+      info[q] = atomicAdd(cnt + map_bucket((unsigned)(keys[q] - mn), mul, H), 1);
+    tile.sync();
+    // -- exclusive scan of the bucket counts (cnt becomes bucket starts)
+    constexpr int PER = H >= G ? H / G : 1;
+    if constexpr (PER <= 8) {
+      int local[PER];
+      int sum = 0;
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int i = lane * PER + q;
+        local[q] = i < H ? cnt[i] : 0;
+        sum += local[q];
+      }
+      int ex = cg::exclusive_scan(tile, sum, cg::plus<int>());
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int i = lane * PER + q;
+        if (i < H) cnt[i] = ex;
+        ex += local[q];
+      }
+    } else {
+      int run = 0;
+      for (int base = 0; base < H; base += G) {
+        const int v = cnt[base + lane];
+        const int incl = cg::inclusive_scan(tile, v, cg::plus<int>());
+        cnt[base + lane] = run + incl - v;
+        run += tile.shfl(incl, G - 1);
+      }
+    }
+    tile.sync();
+    // -- keys in bucket order
+    for (int q = lane; q < n; q += G) {
+      const int key = keys[q];
+      bkey[cnt[map_bucket((unsigned)(key - mn), mul, H)] + info[q]] = key;
+    }
+    tile.sync();
+    // -- rank inside the bucket; store straight to C
+    for (int q = lane; q < n; q += G) {
+      const int key = keys[q];
+      const int b = map_bucket((unsigned)(key - mn), mul, H);
+      const int st = cnt[b], en = b + 1 < H ? cnt[b + 1] : n;
+      int rank = st;
+      for (int u = st; u < en; ++u) rank += bkey[u] < key;
+      __stcs(ccol + c0 + rank, key);
+      __stcs(cval + c0 + rank, vals[q]);
+    }
+    tile.sync();
+    for (int s = lane; s < H / 4; s += G) c4[s] = make_int4(0, 0, 0, 0);
+    tile.sync();
+  }
+}
+
+template <int G, int LOG2H>
+static cudaError_t run_num_map(const ProdTable<double> &t, const unsigned char *map,
+                               const unsigned *map_off, const int *crpt, int *ccol,
+                               double *cval, const int *rows, int count, int *err,
+                               cudaStream_t s) {
+  using C = NumMapCfg<G, LOG2H>;
+  auto kern = t.prod_of_row ? k_num_map<G, LOG2H, true> : k_num_map<G, LOG2H, false>;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, map, map_off, crpt, ccol, cval, rows, count, err);
+  return cudaGetLastError();
+}
+
+template <int G>
+static cudaError_t num_map_bin(int bin, const ProdTable<double> &t, const unsigned char *map,
+                               const unsigned *map_off, const int *crpt, int *ccol,
+                               double *cval, const int *rows, int count, int *err,
+                               cudaStream_t s) {
+#define NSPB_NMAP(L2H) run_num_map<G, L2H>(t, map, map_off, crpt, ccol, cval, rows, count, err, s)
+  switch (bin) {
+    case 0: return NSPB_NMAP(4);
+    case 1: return NSPB_NMAP(5);
+    case 2: return NSPB_NMAP(6);
+    case 3: return NSPB_NMAP(7);
+    default: return NSPB_NMAP(8);
+  }
+#undef NSPB_NMAP
+}
+
+cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
+                               const unsigned char *map, const unsigned *map_off,
+                               const int *crpt, int *ccol, double *cval, const int *rows,
+                               int count, int *err, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (bin >= kMapNumBins) return cudaErrorInvalidValue;
+  if (lanes == 8)
+    return num_map_bin<8>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err, s);
+  if (lanes == 16)
+    return num_map_bin<16>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err, s);
+  return num_map_bin<32>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err, s);
+}
+
+}  // namespace nspb

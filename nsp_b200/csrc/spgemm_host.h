@@ -73,6 +73,17 @@ struct Call {
   size_t ext_bytes = 0;
   bool ws_external = false;
   HostStage *stage = nullptr;
+  // Entry maps (k_sym_map / k_num_map): the symbolic phase records, for each
+  // intermediate product, its column's index among the row's distinct
+  // columns; the numeric row-group bins of at most 256 entries then add every
+  // product at its index with no hash table. allow_map false: entry points
+  // whose numeric phase runs in another call, or that may not allocate.
+  bool allow_map = true;
+  bool use_map = false;
+  void *map_block = nullptr;   // pool block: map_off (n entries), then the map
+  unsigned char *map = nullptr;
+  unsigned *map_off = nullptr;
+  bool map_wanted() const;
   // opts.timing: events around rowinfo, symbolic, scan, numeric
   cudaEvent_t ev[8] = {};
   bool timing = false;

@@ -72,6 +72,182 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---- row groups that also record each product's entry index ------------------
+// Same count as k_sym_group, and an entry map for the numeric phase: for
+// every intermediate product, the index of its column among the row's
+// distinct columns in order of first appearance (one byte). The numeric
+// kernel (k_num_map) then adds every product at its index with no hash probe.
+// The table holds 4-byte slots (column - row's first column) << 8 | index,
+// so a probe returns the index with the key; new columns of a step take
+// consecutive indices from one ballot, so the new columns of a step hold the
+// indices [count before the step, count after it). A group barrier after
+// every step makes its inserts visible to the next: a probe that met a stale
+// empty slot for a key of an earlier step would take a second index for it. Indices past 255 are not
+// recorded (such rows have more than 256 entries and take the hash kernels).
+// Layout of a row's map (map_quad decides, identically in both kernels):
+// A entries in chunks of G; in a chunk, steps (one B row each) go in quads of
+// four while the next four B rows each fit the group and hold at least 3G
+// products together: a quad takes 4G bytes at a 4-byte boundary, lane l's
+// word holding the four steps' bytes of B entry l; from the first step that
+// does not start such a quad to the end of the chunk, each product takes one
+// byte in walk order. Row r of the launch writes its map at
+// map + bin_off + r * stride and its 16-byte unit offset to map_off[row]; a
+// row whose map outgrows stride raises MAP_OVERFLOW in *flags (the host then
+// drops the map).
+template <int G, int LOG2T>
+__device__ __forceinline__ int sym_map_product(unsigned *table, bool has, unsigned rk, int &nk,
+                                               unsigned below,
+                                               const cg::thread_block_tile<G> &tile,
+                                               int *err) {
+  constexpr unsigned MASK = (1u << LOG2T) - 1u;
+  unsigned h = hash_slot<LOG2T>((int)rk);
+  int idx = 0;
+  bool need = false;
+  if (has) {
+    // slots only go from empty to a key: a stale read is a stale empty,
+    // which the CAS below corrects
+    unsigned cur = table[h];
+#pragma unroll 1
+    for (unsigned q = 0;; ++q) {
+      if ((cur >> 8) == rk) {
+        idx = (int)(cur & 0xffu);
+        break;
+      }
+      if (cur == kMapEmpty) {
+        need = true;
+        break;
+      }
+      if (q == MASK) {
+        atomicOr(err, ERR_PROBE);
+        break;
+      }
+      h = (h + 1u) & MASK;
+      cur = table[h];
+    }
+  }
+  // the new columns of the step take consecutive indices in lane order
+  const unsigned nm = tile.ballot(need);
+  const int mine = nk + __popc(nm & below);
+  nk += __popc(nm);
+  if (need) {
+    idx = min(mine, 255);
+    const unsigned packed = (rk << 8) | (unsigned)idx;
+#pragma unroll 1
+    for (unsigned q = 0;; ++q) {
+      // keys of a step are distinct: a lost race was for another key
+      if (atomicCAS(table + h, kMapEmpty, packed) == kMapEmpty) break;
+      if (q == MASK) {
+        atomicOr(err, ERR_PROBE);
+        break;
+      }
+      h = (h + 1u) & MASK;
+    }
+  }
+  return idx;
+}
+
+template <int G, int LOG2T, bool MULTI>
+__global__ void __launch_bounds__(256, 5)
+    k_sym_map(const ProdTable<void> src, const int *__restrict__ rows, int count,
+              int *__restrict__ row_nz, int *__restrict__ err, unsigned char *__restrict__ map,
+              long long bin_off, int stride, unsigned *__restrict__ map_off,
+              int *__restrict__ flags) {
+  using C = SymGroupCfg<G, LOG2T>;
+  extern __shared__ __align__(16) unsigned smem_symm[];
+  auto tile = cg::tiled_partition<G>(cg::this_thread_block());
+  const int g = threadIdx.x / G;
+  const int lane = tile.thread_rank();
+  const unsigned below = (1u << lane) - 1u;
+  unsigned *table = smem_symm + g * C::T;
+  for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
+    const int row = rows ? rows[r] : r;
+    uint4 *t4 = reinterpret_cast<uint4 *>(table);
+#pragma unroll 4
+    for (int s = lane; s < C::T / 4; s += G)
+      t4[s] = make_uint4(kMapEmpty, kMapEmpty, kMapEmpty, kMapEmpty);
+    Operands<void> o;
+    const int lr = prod_row<MULTI>(src, row, o);
+    const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
+    // B row bounds of the first G A entries, and the row's first column
+    int bs = 0, be = 0, mn = 0x7fffffff;
+    if (a0 + lane < a1) {
+      const int k = ld_stream(o.acol + a0 + lane);
+      bs = __ldg(o.brpt + k);
+      be = __ldg(o.brpt + k + 1);
+      if (be > bs) mn = __ldg(o.bcol + bs);
+    }
+    for (int j = a0 + G + lane; j < a1; j += G) {
+      const int k = __ldg(o.acol + j);
+      const int s0 = __ldg(o.brpt + k), s1 = __ldg(o.brpt + k + 1);
+      if (s1 > s0) mn = min(mn, __ldg(o.bcol + s0));
+    }
+    mn = cg::reduce(tile, mn, cg::less<int>());
+    tile.sync();  // the table is clear
+    unsigned char *mp = map + bin_off + (size_t)r * stride;
+    int nk = 0;   // distinct columns so far (uniform across the group)
+    int pos = 0;  // map bytes so far, saturated at stride + 1
+    for (int ab = a0; ab < a1; ab += G) {
+      if (ab > a0) {
+        bs = be = 0;
+        if (ab + lane < a1) {
+          const int k = ld_stream(o.acol + ab + lane);
+          bs = __ldg(o.brpt + k);
+          be = __ldg(o.brpt + k + 1);
+        }
+      }
+      const int cnt = min(G, a1 - ab);
+      int t = 0;
+      // quads: one 4-byte word per lane
+      for (; t + 4 <= cnt; t += 4) {
+        int s0[4], len[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          s0[i] = tile.shfl(bs, t + i);
+          len[i] = tile.shfl(be, t + i) - s0[i];
+        }
+        if (!map_quad<G>(len)) break;
+        unsigned word = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const bool has = lane < len[i];
+          const unsigned rk = has ? (unsigned)(__ldg(o.bcol + s0[i] + lane) - mn) : 0u;
+          const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
+          word |= (unsigned)idx << (8 * i);
+          tile.sync();  // the next step sees this step's inserts
+        }
+        const int pa = (pos + 3) & ~3;
+        if (pa + 4 * G <= stride) reinterpret_cast<unsigned *>(mp + pa)[lane] = word;
+        pos = min(pa + 4 * G, stride + 1);
+      }
+      // the rest of the chunk: one byte per product
+      for (; t < cnt; ++t) {
+        const int s0 = tile.shfl(bs, t), s1 = tile.shfl(be, t);
+        unsigned char *sp = mp + pos - s0;  // sp[e]: the byte of B entry e
+        const int room = stride - pos;
+        for (int eb = s0; eb < s1; eb += G) {  // uniform trip count across the group
+          const int e = eb + lane;
+          const bool has = e < s1;
+          const unsigned rk = has ? (unsigned)(__ldg(o.bcol + e) - mn) : 0u;
+          const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
+          if (has && e - s0 < room) sp[e] = (unsigned char)idx;
+        }
+        pos = (int)min((long long)pos + (s1 - s0), (long long)stride + 1);
+        tile.sync();  // the next step sees this step's inserts
+      }
+    }
+    if (lane == 0) {
+      row_nz[row] = nk;
+      if (pos <= stride) {
+        map_off[row] = (unsigned)((bin_off + (long long)r * stride) >> 4);
+      } else {
+        map_off[row] = kNoMap;
+        atomicOr(flags, MAP_OVERFLOW);
+      }
+    }
+    tile.sync();
+  }
+}
+
 // ---- rows of more than 3072 intermediate products: one block per row ---------
 // Distinct columns are counted as set bits of a shared-memory bitmap over the
 // row's column span [lo, hi] (see row_span), in windows of 2^20 columns. A
@@ -190,6 +366,43 @@ static cudaError_t sym_group_bin(int bin, const ProdTable<void> &t, const int *r
     case 6: return run_sym_group<G, 11>(t, rows, count, row_nz, err, s);
     default: return run_sym_group<G, 12>(t, rows, count, row_nz, err, s);
   }
+}
+
+template <int G, int LOG2T>
+static cudaError_t run_sym_map(const ProdTable<void> &t, const int *rows, int count,
+                               int *row_nz, int *err, const MapArgs &m, cudaStream_t s) {
+  using C = SymGroupCfg<G, LOG2T>;
+  auto kern = t.prod_of_row ? k_sym_map<G, LOG2T, true> : k_sym_map<G, LOG2T, false>;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, rows, count, row_nz, err, m.map, m.bin_off, m.stride,
+                                         m.map_off, m.flags);
+  return cudaGetLastError();
+}
+
+template <int G>
+static cudaError_t sym_map_bin(int bin, const ProdTable<void> &t, const int *rows, int count,
+                               int *row_nz, int *err, const MapArgs &m, cudaStream_t s) {
+  switch (bin) {
+    case 0: return run_sym_map<G, 5>(t, rows, count, row_nz, err, m, s);
+    case 1: return run_sym_map<G, 6>(t, rows, count, row_nz, err, m, s);
+    case 2: return run_sym_map<G, 7>(t, rows, count, row_nz, err, m, s);
+    case 3: return run_sym_map<G, 8>(t, rows, count, row_nz, err, m, s);
+    case 4: return run_sym_map<G, 9>(t, rows, count, row_nz, err, m, s);
+    case 5: return run_sym_map<G, 10>(t, rows, count, row_nz, err, m, s);
+    case 6: return run_sym_map<G, 11>(t, rows, count, row_nz, err, m, s);
+    default: return run_sym_map<G, 12>(t, rows, count, row_nz, err, m, s);
+  }
+}
+
+cudaError_t launch_symbolic_map(int bin, int lanes, const ProdTable<void> &t, const int *rows,
+                                int count, int *row_nz, int *err, const MapArgs &m,
+                                cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (bin >= kSymGroupBins) return cudaErrorInvalidValue;
+  if (lanes == 8) return sym_map_bin<8>(bin, t, rows, count, row_nz, err, m, s);
+  if (lanes == 16) return sym_map_bin<16>(bin, t, rows, count, row_nz, err, m, s);
+  return sym_map_bin<32>(bin, t, rows, count, row_nz, err, m, s);
 }
 
 cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTable<void> &t,
