@@ -127,8 +127,8 @@ typedef struct {
                             <= 256 entries add at that index with no hash
                             table (0 takes maps when the B rows read fill
                             3/4 of the row groups' lanes on average; maps
-                            need fp64, one-call products, sorted B rows, no
-                            row of more than 3072 products, < 2^24 columns) */
+                            need one-call products, sorted B rows, no row of
+                            more than 3072 products, < 2^24 columns)        */
   int32_t sym_fill_pct;  /* symbolic bin thresholds: a row goes to the bin
                             whose table (32 << b slots) it fills to at most
                             this percentage at its upper bound of distinct

@@ -55,12 +55,16 @@ struct NumMapCfg {
   static constexpr int SMEM = GPC * BYTES;
 };
 
-template <int G, int LOG2H, bool MULTI>
+// VT float with COMP: fp32 inputs; rows of at most comp.nmax A entries sum
+// error-free fp32 pairs (TwoProduct + TwoSum) collapsed to fp64 at the end,
+// the others (every row when comp.nmax is 0) sum the exact fp64 products of
+// the widened inputs.
+template <int G, int LOG2H, typename VT, bool COMP, bool MULTI>
 __global__ void __launch_bounds__(256)
-    k_num_map(const ProdTable<double> src, const unsigned char *__restrict__ map,
+    k_num_map(const ProdTable<VT> src, const unsigned char *__restrict__ map,
               const unsigned *__restrict__ map_off, const int *__restrict__ crpt,
               int *__restrict__ ccol, double *__restrict__ cval, const int *__restrict__ rows,
-              int count, int *__restrict__ err) {
+              int count, int *__restrict__ err, CompArgs comp) {
   using C = NumMapCfg<G, LOG2H>;
   constexpr int H = C::H;
   extern __shared__ __align__(16) unsigned char smem_nmap[];
@@ -69,6 +73,7 @@ __global__ void __launch_bounds__(256)
   const int lane = tile.thread_rank();
   unsigned char *gb = smem_nmap + (size_t)g * C::BYTES;
   double *vals = reinterpret_cast<double *>(gb);
+  float2 *vals2 = reinterpret_cast<float2 *>(gb);  // the same 8 bytes as fp32 pairs
   int *keys = reinterpret_cast<int *>(gb + (size_t)H * 8);
   int *info = keys + H;
   int *cnt = info + H;
@@ -78,6 +83,7 @@ __global__ void __launch_bounds__(256)
   for (int s = lane; s < H / 4; s += G) c4[s] = make_int4(0, 0, 0, 0);
   tile.sync();
 
+  int my_max_deg = 0, my_redo = 0;  // compensated mode, flushed once per group
   for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
     const int row = rows ? rows[r] : r;
     const int c0 = crpt[row];
@@ -89,11 +95,12 @@ __global__ void __launch_bounds__(256)
       continue;
     }
     const unsigned char *mp = map + (size_t)mo * 16;
-    Operands<double> op;
+    Operands<VT> op;
     const int lr = prod_row<MULTI>(src, row, op);
     const int *acol = op.acol, *brpt = op.brpt, *bcol = op.bcol;
-    const double *aval = op.aval, *bval = op.bval;
+    const VT *aval = op.aval, *bval = op.bval;
     const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
+    const bool pair = COMP && (a1 - a0) <= comp.nmax;
     int mn = 0x7fffffff, mx = -1;
     int nk = 0;   // distinct columns before the current step (uniform)
     int pos = 0;  // products walked so far (uniform)
@@ -101,18 +108,28 @@ __global__ void __launch_bounds__(256)
     // hold the indices from nk on; nf counts them within the step.
     bool bad = false;
     int nf = 0;
-    auto add = [&](bool has, unsigned ix, int c, double p) {
+    auto add = [&](bool has, unsigned ix, int c, double a, double b) {
       if (has && ix >= (unsigned)n) {  // not an index of this row: corrupt map
         bad = true;
         has = false;
       }
       const bool fresh = has && (int)ix >= nk;
       nf += __popc(tile.ballot(fresh));
-      if (fresh) {
-        keys[ix] = c;
-        vals[ix] = __dadd_rn(0.0, p);
-      } else if (has) {
-        vals[ix] = __dadd_rn(vals[ix], p);
+      if (fresh) keys[ix] = c;
+      if (!has) return;
+      if (pair) {  // a and b hold fp32 values: the conversions are exact
+        const float af = (float)a, bf = (float)b;
+        if (fresh) {
+          const float ph = __fmul_rn(af, bf);
+          vals2[ix] = make_float2(ph, __fmaf_rn(af, bf, -ph));
+        } else {
+          float2 sc = vals2[ix];
+          comp_add(sc, af, bf);
+          vals2[ix] = sc;
+        }
+      } else {
+        const double p = __dmul_rn(a, b);
+        vals[ix] = __dadd_rn(fresh ? 0.0 : vals[ix], p);
       }
     };
     for (int ab = a0; ab < a1; ab += G) {
@@ -156,11 +173,11 @@ __global__ void __launch_bounds__(256)
             const bool has = lane < len[i];
             ix[i] = (w >> (8 * i)) & 0xffu;
             kc[i] = has ? __ldg(bcol + e) : 0;
-            b[i] = has ? __ldg(bval + e) : 0.0;
+            b[i] = has ? ldv(bval + e) : 0.0;
           }
 #pragma unroll
           for (int i = 0; i < D; ++i) {
-            add(lane < len[i], ix[i], kc[i], __dmul_rn(__hiloint2double(q[i].w, q[i].z), b[i]));
+            add(lane < len[i], ix[i], kc[i], __hiloint2double(q[i].w, q[i].z), b[i]);
             nk += nf;
             nf = 0;
             tile.sync();  // the next step may hit the same entries
@@ -187,13 +204,12 @@ __global__ void __launch_bounds__(256)
           const bool has = e < q[i].y;
           ix[i] = has ? ld_stream(mp + pos + lane) : 0u;
           kc[i] = has ? __ldg(bcol + e) : 0;
-          b[i] = has ? __ldg(bval + e) : 0.0;
+          b[i] = has ? ldv(bval + e) : 0.0;
           pos += q[i].y - q[i].x;
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          add(q[i].x + lane < q[i].y, ix[i], kc[i],
-              __dmul_rn(__hiloint2double(q[i].w, q[i].z), b[i]));
+          add(q[i].x + lane < q[i].y, ix[i], kc[i], __hiloint2double(q[i].w, q[i].z), b[i]);
           nk += nf;
           nf = 0;
           tile.sync();  // the next step may hit the same entries
@@ -207,8 +223,8 @@ __global__ void __launch_bounds__(256)
           const bool has = e < q.y;
           const unsigned ix = has ? ld_stream(mp + pos + (e - q.x)) : 0u;
           const int kc = has ? __ldg(bcol + e) : 0;
-          const double bv = has ? __ldg(bval + e) : 0.0;
-          add(has, ix, kc, __dmul_rn(a, bv));
+          const double bv = has ? ldv(bval + e) : 0.0;
+          add(has, ix, kc, a, bv);
         }
         pos += q.y - q.x;
         nk += nf;
@@ -269,34 +285,52 @@ __global__ void __launch_bounds__(256)
       const int st = cnt[b], en = b + 1 < H ? cnt[b + 1] : n;
       int rank = st;
       for (int u = st; u < en; ++u) rank += bkey[u] < key;
+      double v;
+      if (pair) {
+        const float2 sc = vals2[q];
+        v = (double)sc.x + (double)sc.y;
+      } else {
+        v = vals[q];
+      }
       __stcs(ccol + c0 + rank, key);
-      __stcs(cval + c0 + rank, vals[q]);
+      __stcs(cval + c0 + rank, v);
+    }
+    if (COMP) {
+      if (pair) my_max_deg = max(my_max_deg, a1 - a0);
+      else ++my_redo;
     }
     tile.sync();
     for (int s = lane; s < H / 4; s += G) c4[s] = make_int4(0, 0, 0, 0);
     tile.sync();
   }
+  if (COMP && lane == 0) {
+    if (my_max_deg) atomicMax(comp.max_deg, my_max_deg);
+    if (my_redo) atomicAdd(comp.redo, my_redo);
+  }
 }
 
-template <int G, int LOG2H>
-static cudaError_t run_num_map(const ProdTable<double> &t, const unsigned char *map,
+template <int G, int LOG2H, typename VT, bool COMP>
+static cudaError_t run_num_map(const ProdTable<VT> &t, const unsigned char *map,
                                const unsigned *map_off, const int *crpt, int *ccol,
-                               double *cval, const int *rows, int count, int *err,
+                               double *cval, const int *rows, int count, int *err, CompArgs comp,
                                cudaStream_t s) {
   using C = NumMapCfg<G, LOG2H>;
-  auto kern = t.prod_of_row ? k_num_map<G, LOG2H, true> : k_num_map<G, LOG2H, false>;
+  auto kern = t.prod_of_row ? k_num_map<G, LOG2H, VT, COMP, true>
+                            : k_num_map<G, LOG2H, VT, COMP, false>;
   const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
-  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, map, map_off, crpt, ccol, cval, rows, count, err);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(t, map, map_off, crpt, ccol, cval, rows, count, err,
+                                         comp);
   return cudaGetLastError();
 }
 
-template <int G>
-static cudaError_t num_map_bin(int bin, const ProdTable<double> &t, const unsigned char *map,
+template <int G, typename VT, bool COMP>
+static cudaError_t num_map_bin(int bin, const ProdTable<VT> &t, const unsigned char *map,
                                const unsigned *map_off, const int *crpt, int *ccol,
-                               double *cval, const int *rows, int count, int *err,
+                               double *cval, const int *rows, int count, int *err, CompArgs comp,
                                cudaStream_t s) {
-#define NSPB_NMAP(L2H) run_num_map<G, L2H>(t, map, map_off, crpt, ccol, cval, rows, count, err, s)
+#define NSPB_NMAP(L2H) \
+  run_num_map<G, L2H, VT, COMP>(t, map, map_off, crpt, ccol, cval, rows, count, err, comp, s)
   switch (bin) {
     case 0: return NSPB_NMAP(4);
     case 1: return NSPB_NMAP(5);
@@ -313,11 +347,33 @@ cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
                                int count, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin >= kMapNumBins) return cudaErrorInvalidValue;
+  const CompArgs none{0, nullptr, nullptr};
   if (lanes == 8)
-    return num_map_bin<8>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err, s);
+    return num_map_bin<8, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count,
+                                         err, none, s);
   if (lanes == 16)
-    return num_map_bin<16>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err, s);
-  return num_map_bin<32>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err, s);
+    return num_map_bin<16, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count,
+                                          err, none, s);
+  return num_map_bin<32, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
+                                        none, s);
+}
+
+cudaError_t launch_numeric_comp_map(int bin, int lanes, const ProdTable<float> &t,
+                                    const unsigned char *map, const unsigned *map_off,
+                                    const int *crpt, int *ccol, double *cval, const int *rows,
+                                    int count, int nmax, int *redo, int *max_deg, int *err,
+                                    cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  if (bin >= kMapNumBins) return cudaErrorInvalidValue;
+  const CompArgs comp{nmax, redo, max_deg};
+  if (lanes == 8)
+    return num_map_bin<8, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
+                                       comp, s);
+  if (lanes == 16)
+    return num_map_bin<16, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
+                                        comp, s);
+  return num_map_bin<32, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
+                                      comp, s);
 }
 
 }  // namespace nspb

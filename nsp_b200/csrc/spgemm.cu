@@ -414,9 +414,11 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     const int *rows = direct ? nullptr : perm + off.v[b];
     int *ticket = &ctr->ticket[16 + b];
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
-    if (use_map && b < kMapNumBins && !comp) {
-      e = launch_numeric_map(b, lanes, t64, map, map_off, crpt, ccol, cval, rows, c, &ctr->err,
-                             s);
+    if (use_map && b < kMapNumBins) {
+      e = comp ? launch_numeric_comp_map(b, lanes, t32, map, map_off, crpt, ccol, cval, rows, c,
+                                         nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
+               : launch_numeric_map(b, lanes, t64, map, map_off, crpt, ccol, cval, rows, c,
+                                    &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;
       continue;
@@ -447,7 +449,7 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
 }
 
 // The symbolic phase records entry maps when the numeric phase of the same
-// call can use them: fp64, B rows strictly increasing, every row with
+// call can use them: B rows strictly increasing, every row with
 // products in a row-group symbolic bin, column offsets within 24 bits, and
 // row_kernel 7 (maps), or 0 (automatic) when the B rows the products read
 // fill at least 3/4 of a row group's lanes on average. The map costs the
@@ -461,7 +463,7 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
 bool Call::map_wanted() const {
   const int k = opts.row_kernel & 0xff;
   if (!allow_map || !(k == 0 || k == 7)) return false;
-  if (opts.precision != NSPB_PREC_FP64 || !b_sorted || n <= 0 || a_nnz <= 0) return false;
+  if (!b_sorted || n <= 0 || a_nnz <= 0) return false;
   if (info.max_ncols > kMapMaxCols) return false;
   for (int b = kSymGroupBins; b < kSymBins; ++b)
     if (h.sym_counts[b] > 0) return false;

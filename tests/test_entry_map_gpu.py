@@ -115,3 +115,38 @@ def test_plan_replays_from_maps(cuda):
     rp, col, val = oracle.spgemm(A, A)
     got = plan.C[0].val.cpu().numpy()
     assert_bitwise(got, 0.25 * val)
+
+
+def _as32(h):
+    return HostCSR(h.nrows, h.ncols, h.rowptr, h.col, h.val.astype(np.float32))
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp32w"])
+def test_fp32_forms_from_maps(cuda, precision):
+    # fp32 values: compensated pairs (fp32c) or exact fp64 products (fp32w),
+    # against the fp64 oracle on the same fp32-representable values
+    A = nb.gen.stencil(30, npts=27, fp32=True)
+    d = _as32(A).to_device()
+    C, st = nb.spgemm(d, d, precision=precision, return_stats=True)
+    got = C.to_host()
+    rp, col, val = oracle.spgemm(A, A)
+    assert_same_structure(got.rowptr, got.col, rp, col)
+    assert st["entry_map"] == 1
+    if precision == "fp32w":  # products exact in fp64, summed in A-row order
+        assert_bitwise(got.val, val)
+    else:
+        bound = oracle.absbound(A, A, rp, col)
+        assert_close(got.val, val, bound, tol=1e-10)
+        err = float(np.max(np.abs(got.val - val) / np.maximum(bound, 1e-300)))
+        assert st["rows_redone"] == 0 and err <= st["max_row_err"] + 1e-15
+
+
+def test_fp32c_maps_rows_over_the_bound_in_fp64(cuda):
+    A = nb.gen.stencil(12, npts=27, fp32=True)
+    d = _as32(A).to_device()
+    C, st = nb.spgemm(d, d, precision="fp32c", comp_tol=1e-15, row_kernel=7, return_stats=True)
+    rp, col, val = oracle.spgemm(A, A)
+    got = C.to_host()
+    assert_same_structure(got.rowptr, got.col, rp, col)
+    assert st["entry_map"] == 1 and st["rows_redone"] == A.nrows
+    assert_bitwise(got.val, val)
