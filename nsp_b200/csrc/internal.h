@@ -232,15 +232,17 @@ cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth,
 // ---- rowmap.cu ------------------------------------------------------------------
 // Numeric row-group bin (bin < kMapNumBins) from the entry maps of a
 // map-recording symbolic phase: no hash table; B rows strictly increasing.
+// prefetch_a (single products only): cp.async copies each group's next row's
+// first A entries into shared memory while the current row is computed.
 cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
                                const unsigned char *map, const unsigned *map_off,
                                const int *crpt, int *ccol, double *cval, const int *rows,
-                               int count, int *err, cudaStream_t s);
+                               int count, bool prefetch_a, int *err, cudaStream_t s);
 // The same for fp32 inputs: rows of at most nmax A entries in fp32 pairs, the
 // others in fp64 from exact products (see launch_numeric_comp_bin).
 cudaError_t launch_numeric_comp_map(int bin, int lanes, const ProdTable<float> &t,
                                     const unsigned char *map, const unsigned *map_off,
                                     const int *crpt, int *ccol, double *cval, const int *rows,
-                                    int count, int nmax, int *redo, int *max_deg, int *err,
-                                    cudaStream_t s);
+                                    int count, bool prefetch_a, int nmax, int *redo,
+                                    int *max_deg, int *err, cudaStream_t s);
 }  // namespace nspb

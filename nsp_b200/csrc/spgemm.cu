@@ -415,9 +415,14 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
     int *ticket = &ctr->ticket[16 + b];
     const int tshift = opts.num_table_shift == 1 ? 1 : 0;
     if (use_map && b < kMapNumBins) {
+      // cp.async of the next row's A entries pays on short A rows (7-point
+      // Laplacian 128^3: numeric 1.47 -> 1.16 ms) and costs on long ones
+      // (27-point stencil 128^3: 6.63 -> 7.42 ms, L1 data pipe saturated)
+      const bool pref = !table && a_nnz <= 12LL * n;
       e = comp ? launch_numeric_comp_map(b, lanes, t32, map, map_off, crpt, ccol, cval, rows, c,
-                                         nmax, &ctr->redo_count, &ctr->max_comp_deg, &ctr->err, s)
-               : launch_numeric_map(b, lanes, t64, map, map_off, crpt, ccol, cval, rows, c,
+                                         pref, nmax, &ctr->redo_count, &ctr->max_comp_deg,
+                                         &ctr->err, s)
+               : launch_numeric_map(b, lanes, t64, map, map_off, crpt, ccol, cval, rows, c, pref,
                                     &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;
