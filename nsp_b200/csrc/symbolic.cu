@@ -82,8 +82,9 @@ __global__ void __launch_bounds__(256)
 // consecutive indices from one ballot, so the new columns of a step hold the
 // indices [count before the step, count after it). A group barrier after
 // every step makes its inserts visible to the next: a probe that met a stale
-// empty slot for a key of an earlier step would take a second index for it. Indices past 255 are not
-// recorded (such rows have more than 256 entries and take the hash kernels).
+// empty slot for a key of an earlier step would take a second index for it.
+// Indices past 255 are not recorded (such rows have more than 256 entries
+// and take the hash kernels).
 // Layout of a row's map (map_quad decides, identically in both kernels):
 // A entries in chunks of G; in a chunk, steps (one B row each) go in quads of
 // four while the next four B rows each fit the group and hold at least 3G
@@ -206,11 +207,17 @@ __global__ void __launch_bounds__(256, 5)
           len[i] = tile.shfl(be, t + i) - s0[i];
         }
         if (!map_quad<G>(len)) break;
+        // the four B rows' columns are loaded before the first insert (the
+        // group barrier of each step would otherwise hold the next load back)
+        unsigned rks[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          rks[i] = lane < len[i] ? (unsigned)(__ldg(o.bcol + s0[i] + lane) - mn) : 0u;
         unsigned word = 0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const bool has = lane < len[i];
-          const unsigned rk = has ? (unsigned)(__ldg(o.bcol + s0[i] + lane) - mn) : 0u;
+          const unsigned rk = rks[i];
           const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
           word |= (unsigned)idx << (8 * i);
           tile.sync();  // the next step sees this step's inserts
