@@ -116,7 +116,12 @@ struct MapArgs {
   int stride = 0;                // bytes per row (a multiple of 16)
   unsigned *map_off = nullptr;   // per global row
   int *flags = nullptr;          // MAP_OVERFLOW
+  int chunk = 1;                 // rows a group takes in a run; > 1: row templates
 };
+// Row templates of the map symbolic pass: consecutive rows a group takes in a
+// run, and the opts.row_kernel bit that turns templates off.
+constexpr int kTemplateRun = 16;
+constexpr int kNoRowTemplates = 0x10000;
 
 // fp32 input modes (compensated pairs, or fp64 accumulation of exact products).
 inline bool fp32_inputs(int precision) {
@@ -234,15 +239,17 @@ cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth,
 // map-recording symbolic phase: no hash table; B rows strictly increasing.
 // prefetch_a (single products only): cp.async copies each group's next row's
 // first A entries into shared memory while the current row is computed.
+// run > 1: groups take runs of `run` consecutive rows and reuse the sort of a
+// row for the rows that share its map (row templates of the symbolic pass).
 cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
                                const unsigned char *map, const unsigned *map_off,
                                const int *crpt, int *ccol, double *cval, const int *rows,
-                               int count, bool prefetch_a, int *err, cudaStream_t s);
+                               int count, bool prefetch_a, int run, int *err, cudaStream_t s);
 // The same for fp32 inputs: rows of at most nmax A entries in fp32 pairs, the
 // others in fp64 from exact products (see launch_numeric_comp_bin).
 cudaError_t launch_numeric_comp_map(int bin, int lanes, const ProdTable<float> &t,
                                     const unsigned char *map, const unsigned *map_off,
                                     const int *crpt, int *ccol, double *cval, const int *rows,
-                                    int count, bool prefetch_a, int nmax, int *redo,
+                                    int count, bool prefetch_a, int run, int nmax, int *redo,
                                     int *max_deg, int *err, cudaStream_t s);
 }  // namespace nspb

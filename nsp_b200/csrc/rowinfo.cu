@@ -218,27 +218,43 @@ cudaError_t launch_rowinfo(const ProdTable<void> &t, int n, int64_t a_nnz, const
 }
 
 // ---- bin permutation ------------------------------------------------------------
+// Each block of 1024 rows lists its rows of every bin in ascending row order
+// (a stable split: ranks inside a warp from __match_any_sync peers, warp
+// offsets from a scan of the per-warp counts), at a place in the bin that one
+// atomic per (block, bin) reserves. Runs of consecutive list entries are then
+// runs of neighbouring rows, which the row templates of the entry-map kernels
+// rely on (rows of a structured grid repeat their neighbours' pattern).
 __global__ void __launch_bounds__(1024)
     k_perm(const int *__restrict__ key, int n, int kind, BinOffsets off, const BinLimits lim,
            int *__restrict__ cursor, int *__restrict__ perm) {
-  __shared__ int hist[16];
+  __shared__ int wcnt[16][33];  // [bin][warp]: rows, then the warp's offset in the block
   __shared__ int base[16];
-  if (threadIdx.x < 16) hist[threadIdx.x] = 0;
-  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = threadIdx.x; t < 16 * 33; t += blockDim.x) (&wcnt[0][0])[t] = 0;
   const int i = blockIdx.x * 1024 + threadIdx.x;
-  int b = -1, r = 0;
+  int b = -1;
   if (i < n) {
     const int k = kind == 0 ? key[i] : key[i + 1] - key[i];
-    if (k > 0) {
-      b = kind == 0 ? sym_bin(k, lim) : num_bin(k, lim);
-      r = atomicAdd(&hist[b], 1);
-    }
+    if (k > 0) b = kind == 0 ? sym_bin(k, lim) : num_bin(k, lim);
   }
   __syncthreads();
-  if (threadIdx.x < 16 && hist[threadIdx.x])
-    base[threadIdx.x] = off.v[threadIdx.x] + atomicAdd(&cursor[threadIdx.x], hist[threadIdx.x]);
+  const unsigned peers = __match_any_sync(0xffffffffu, b);
+  const int rank = __popc(peers & ((1u << lane) - 1u));
+  if (b >= 0 && rank == 0) wcnt[b][w] = __popc(peers);
   __syncthreads();
-  if (b >= 0) perm[base[b] + r] = i;
+  if (w < 16) {  // warp w scans bin w over the block's 32 warps
+    const int v = wcnt[w][lane];
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    wcnt[w][lane] = incl - v;
+    if (lane == 31 && incl > 0) base[w] = off.v[w] + atomicAdd(&cursor[w], incl);
+  }
+  __syncthreads();
+  if (b >= 0) perm[base[b] + wcnt[b][w] + rank] = i;
 }
 
 cudaError_t launch_perm(const int *key, int n, int kind, BinOffsets offsets, const BinLimits &lim,

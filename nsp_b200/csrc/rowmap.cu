@@ -47,11 +47,25 @@ __device__ __forceinline__ int map_bucket(unsigned r, unsigned mul, int nb) {
 // stored at its ranks.
 // Per group: vals[H] fp64, keys[H], info[H] (index inside the bucket), cnt[H],
 // bkey[H] (keys in bucket order), stage[G]; with PREF two buffers of G A
-// entries (values, then columns) that cp.async fills for the group's next row.
+// entries (values, then columns) that cp.async fills for the group's next row;
+// then the row template: trel[H] (its columns in order, less its first
+// column) and tinv[H] (the entry index of each rank).
+//
+// Row templates (run > 1): groups take their rows in runs of `run`
+// consecutive launch rows. A row whose map offset equals the offset of the
+// last row the group sorted has that row's pattern (the symbolic pass gave
+// both rows one map only after checking every product column against the
+// template's, shift for shift), so the sort's outcome carries over: the
+// group adds the products into zeroed values at their indices, with no
+// column loads, no first-appearance tracking and no sort, and stores entry
+// tinv[q] at rank q with column trel[q] + the row's first column. Sums run in
+// the same order from the same zero, so the values are bit for bit those of
+// a sorted row.
 template <int G, int LOG2H, bool PREF>
 struct NumMapCfg {
   static constexpr int H = 1 << LOG2H;
-  static constexpr int BYTES = (H * 8 + H * 16 + G * 16 + (PREF ? G * 24 : 0) + 15) & ~15;
+  static constexpr int BYTES =
+      (H * 8 + H * 16 + G * 16 + (PREF ? G * 24 : 0) + H * 5 + 15) & ~15;
   static constexpr int kBySmem = (56 * 1024) / BYTES > 0 ? (56 * 1024) / BYTES : 1;
   static constexpr int GPC = kBySmem < 256 / G ? kBySmem : 256 / G;
   static constexpr int THREADS = GPC * G;
@@ -74,7 +88,7 @@ __global__ void __launch_bounds__(256)
     k_num_map(const ProdTable<VT> src, const unsigned char *__restrict__ map,
               const unsigned *__restrict__ map_off, const int *__restrict__ crpt,
               int *__restrict__ ccol, double *__restrict__ cval, const int *__restrict__ rows,
-              int count, int *__restrict__ err, CompArgs comp) {
+              int count, int *__restrict__ err, CompArgs comp, int run) {
   static_assert(!(PREF && MULTI), "prefetch serves single products");
   using C = NumMapCfg<G, LOG2H, PREF>;
   constexpr int H = C::H;
@@ -92,12 +106,22 @@ __global__ void __launch_bounds__(256)
   int4 *stage = reinterpret_cast<int4 *>(bkey + H);
   double *avp = reinterpret_cast<double *>(stage + G);  // PREF: [2][G] A values
   int *acp = reinterpret_cast<int *>(avp + 2 * G);      // PREF: [2][G] A columns
+  int *trel = reinterpret_cast<int *>(gb + (size_t)H * 24 + (size_t)G * 16 + (PREF ? G * 24 : 0));
+  unsigned char *tinv = reinterpret_cast<unsigned char *>(trel + H);
   int4 *c4 = reinterpret_cast<int4 *>(cnt);
+  // the group's template: map offset and entries of the last row it sorted
+  unsigned t_mo = kNoMap;
+  int t_n = -1;
   for (int s = lane; s < H / 4; s += G) c4[s] = make_int4(0, 0, 0, 0);
   tile.sync();
 
   int my_max_deg = 0, my_redo = 0;  // compensated mode, flushed once per group
-  const int rstep = gridDim.x * C::GPC;
+  const int rstep = gridDim.x * C::GPC;  // groups in the grid
+  // the group's next launch row after r: the next in its run, else the
+  // first of its next run
+  auto next_r = [&](int r) {
+    return (r + 1) % run != 0 ? r + 1 : (r / run + rstep) * run;
+  };
   // PREF: the first G A entries of the group's row rr into buffer bi
   auto prefetch = [&](int rr, int bi) {
     if constexpr (PREF) {
@@ -114,10 +138,11 @@ __global__ void __launch_bounds__(256)
     }
   };
   int buf = 0;
-  prefetch(blockIdx.x * C::GPC + g, 0);
-  for (int r = blockIdx.x * C::GPC + g; r < count; r += rstep, buf ^= 1) {
+  const int r0 = (blockIdx.x * C::GPC + g) * run;
+  prefetch(r0, 0);
+  for (int r = r0; r < count; r = next_r(r), buf ^= 1) {
     if constexpr (PREF) {
-      prefetch(r + rstep, buf ^ 1);  // the buffer the previous row read
+      prefetch(next_r(r), buf ^ 1);  // the buffer the previous row read
       __pipeline_wait_prior(1);      // this row's copies have landed
       tile.sync();                   // ... for every lane of the group
     }
@@ -137,6 +162,12 @@ __global__ void __launch_bounds__(256)
     const VT *aval = op.aval, *bval = op.bval;
     const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     const bool pair = COMP && (a1 - a0) <= comp.nmax;
+    // a row of the template: no columns, no first appearances, no sort
+    const bool hit = run > 1 && !pair && mo == t_mo && n == t_n;
+    if (hit) {
+      for (int q = lane; q < n; q += G) vals[q] = 0.0;
+      tile.sync();
+    }
     int mn = 0x7fffffff, mx = -1;
     int nk = 0;   // distinct columns before the current step (uniform)
     int pos = 0;  // products walked so far (uniform)
@@ -148,6 +179,10 @@ __global__ void __launch_bounds__(256)
       if (has && ix >= (unsigned)n) {  // not an index of this row: corrupt map
         bad = true;
         has = false;
+      }
+      if (hit) {
+        if (has) vals[ix] = __dadd_rn(vals[ix], __dmul_rn(a, b));
+        return;
       }
       const bool fresh = has && (int)ix >= nk;
       nf += __popc(tile.ballot(fresh));
@@ -215,7 +250,7 @@ __global__ void __launch_bounds__(256)
             const int e = q[i].x + lane;
             const bool has = lane < len[i];
             ix[i] = (w >> (8 * i)) & 0xffu;
-            kc[i] = has ? __ldg(bcol + e) : 0;
+            kc[i] = has && !hit ? __ldg(bcol + e) : 0;
             b[i] = has ? ldv(bval + e) : 0.0;
           }
 #pragma unroll
@@ -246,7 +281,7 @@ __global__ void __launch_bounds__(256)
           const int e = q[i].x + lane;
           const bool has = e < q[i].y;
           ix[i] = has ? ld_stream(mp + pos + lane) : 0u;
-          kc[i] = has ? __ldg(bcol + e) : 0;
+          kc[i] = has && !hit ? __ldg(bcol + e) : 0;
           b[i] = has ? ldv(bval + e) : 0.0;
           pos += q[i].y - q[i].x;
         }
@@ -265,7 +300,7 @@ __global__ void __launch_bounds__(256)
           const int e = eb + lane;
           const bool has = e < q.y;
           const unsigned ix = has ? ld_stream(mp + pos + (e - q.x)) : 0u;
-          const int kc = has ? __ldg(bcol + e) : 0;
+          const int kc = has && !hit ? __ldg(bcol + e) : 0;
           const double bv = has ? ldv(bval + e) : 0.0;
           add(has, ix, kc, a, bv);
         }
@@ -276,6 +311,19 @@ __global__ void __launch_bounds__(256)
       }
     }
     mn = cg::reduce(tile, mn, cg::less<int>());
+    if (hit) {
+      if (tile.any(bad)) {
+        if (lane == 0) atomicOr(err, ERR_COUNT);
+      } else {
+        for (int q = lane; q < n; q += G) {
+          __stcs(ccol + c0 + q, trel[q] + mn);
+          __stcs(cval + c0 + q, vals[tinv[q]]);
+        }
+        if (COMP) ++my_redo;  // a row of fp64 sums (templates never hold pairs)
+      }
+      tile.sync();
+      continue;
+    }
     mx = cg::reduce(tile, mx, cg::greater<int>());
     if (tile.any(bad) || nk != n) {  // map and row pointer disagree: skip the row
       if (lane == 0) atomicOr(err, ERR_COUNT);
@@ -306,12 +354,12 @@ __global__ void __launch_bounds__(256)
         ex += local[q];
       }
     } else {
-      int run = 0;
+      int acc = 0;
       for (int base = 0; base < H; base += G) {
         const int v = cnt[base + lane];
         const int incl = cg::inclusive_scan(tile, v, cg::plus<int>());
-        cnt[base + lane] = run + incl - v;
-        run += tile.shfl(incl, G - 1);
+        cnt[base + lane] = acc + incl - v;
+        acc += tile.shfl(incl, G - 1);
       }
     }
     tile.sync();
@@ -337,7 +385,14 @@ __global__ void __launch_bounds__(256)
       }
       __stcs(ccol + c0 + rank, key);
       __stcs(cval + c0 + rank, v);
+      if (run > 1) {
+        trel[rank] = key - mn;
+        tinv[rank] = (unsigned char)q;
+      }
     }
+    // the sorted row is the template of the rows that share its map
+    t_mo = run > 1 && !pair ? mo : kNoMap;
+    t_n = n;
     if (COMP) {
       if (pair) my_max_deg = max(my_max_deg, a1 - a0);
       else ++my_redo;
@@ -357,13 +412,15 @@ template <int G, int LOG2H, typename VT, bool COMP, bool MULTI, bool PREF>
 static cudaError_t run_num_map_k(const ProdTable<VT> &t, const unsigned char *map,
                                  const unsigned *map_off, const int *crpt, int *ccol,
                                  double *cval, const int *rows, int count, int *err,
-                                 CompArgs comp, cudaStream_t s) {
+                                 CompArgs comp, int run, cudaStream_t s) {
   using C = NumMapCfg<G, LOG2H, PREF>;
   auto kern = k_num_map<G, LOG2H, VT, COMP, MULTI, PREF>;
-  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
+  run = run > 1 ? run : 1;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM,
+                                   (count + run - 1) / run, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, C::THREADS, C::SMEM, s>>>(t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                         comp);
+                                         comp, run);
   return cudaGetLastError();
 }
 
@@ -371,25 +428,25 @@ template <int G, int LOG2H, typename VT, bool COMP>
 static cudaError_t run_num_map(const ProdTable<VT> &t, const unsigned char *map,
                                const unsigned *map_off, const int *crpt, int *ccol,
                                double *cval, const int *rows, int count, int *err, CompArgs comp,
-                               bool pref, cudaStream_t s) {
+                               bool pref, int run, cudaStream_t s) {
   if (t.prod_of_row)
     return run_num_map_k<G, LOG2H, VT, COMP, true, false>(t, map, map_off, crpt, ccol, cval,
-                                                          rows, count, err, comp, s);
+                                                          rows, count, err, comp, run, s);
   if (pref)
     return run_num_map_k<G, LOG2H, VT, COMP, false, true>(t, map, map_off, crpt, ccol, cval,
-                                                          rows, count, err, comp, s);
+                                                          rows, count, err, comp, run, s);
   return run_num_map_k<G, LOG2H, VT, COMP, false, false>(t, map, map_off, crpt, ccol, cval, rows,
-                                                         count, err, comp, s);
+                                                         count, err, comp, run, s);
 }
 
 template <int G, typename VT, bool COMP>
 static cudaError_t num_map_bin(int bin, const ProdTable<VT> &t, const unsigned char *map,
                                const unsigned *map_off, const int *crpt, int *ccol,
                                double *cval, const int *rows, int count, int *err, CompArgs comp,
-                               bool pref, cudaStream_t s) {
+                               bool pref, int run, cudaStream_t s) {
 #define NSPB_NMAP(L2H) \
   run_num_map<G, L2H, VT, COMP>(t, map, map_off, crpt, ccol, cval, rows, count, err, comp, pref, \
-                                s)
+                                run, s)
   switch (bin) {
     case 0: return NSPB_NMAP(4);
     case 1: return NSPB_NMAP(5);
@@ -403,36 +460,36 @@ static cudaError_t num_map_bin(int bin, const ProdTable<VT> &t, const unsigned c
 cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
                                const unsigned char *map, const unsigned *map_off,
                                const int *crpt, int *ccol, double *cval, const int *rows,
-                               int count, bool prefetch_a, int *err, cudaStream_t s) {
+                               int count, bool prefetch_a, int run, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin >= kMapNumBins) return cudaErrorInvalidValue;
   const CompArgs none{0, nullptr, nullptr};
   if (lanes == 8)
     return num_map_bin<8, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count,
-                                         err, none, prefetch_a, s);
+                                         err, none, prefetch_a, run, s);
   if (lanes == 16)
     return num_map_bin<16, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count,
-                                          err, none, prefetch_a, s);
+                                          err, none, prefetch_a, run, s);
   return num_map_bin<32, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                        none, prefetch_a, s);
+                                        none, prefetch_a, run, s);
 }
 
 cudaError_t launch_numeric_comp_map(int bin, int lanes, const ProdTable<float> &t,
                                     const unsigned char *map, const unsigned *map_off,
                                     const int *crpt, int *ccol, double *cval, const int *rows,
-                                    int count, bool prefetch_a, int nmax, int *redo,
+                                    int count, bool prefetch_a, int run, int nmax, int *redo,
                                     int *max_deg, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin >= kMapNumBins) return cudaErrorInvalidValue;
   const CompArgs comp{nmax, redo, max_deg};
   if (lanes == 8)
     return num_map_bin<8, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                       comp, prefetch_a, s);
+                                       comp, prefetch_a, run, s);
   if (lanes == 16)
     return num_map_bin<16, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                        comp, prefetch_a, s);
+                                        comp, prefetch_a, run, s);
   return num_map_bin<32, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                      comp, prefetch_a, s);
+                                      comp, prefetch_a, run, s);
 }
 
 }  // namespace nspb

@@ -359,6 +359,7 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
       m.stride = map_stride[b];
       m.map_off = map_off;
       m.flags = &ctr->flags;
+      m.chunk = opts.row_kernel & kNoRowTemplates ? 1 : kTemplateRun;
       e = launch_symbolic_map(b, lanes, structure_of(t64), rows, c, row_nz, &ctr->err, m, s);
     } else {
       e = launch_symbolic_bin(b, lanes, b_sorted, structure_of(t64), info, rows, c, row_nz,
@@ -419,11 +420,12 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
       // Laplacian 128^3: numeric 1.47 -> 1.16 ms) and costs on long ones
       // (27-point stencil 128^3: 6.63 -> 7.42 ms, L1 data pipe saturated)
       const bool pref = !table && a_nnz <= 12LL * n;
+      const int run = opts.row_kernel & kNoRowTemplates ? 1 : kTemplateRun;
       e = comp ? launch_numeric_comp_map(b, lanes, t32, map, map_off, crpt, ccol, cval, rows, c,
-                                         pref, nmax, &ctr->redo_count, &ctr->max_comp_deg,
+                                         pref, run, nmax, &ctr->redo_count, &ctr->max_comp_deg,
                                          &ctr->err, s)
                : launch_numeric_map(b, lanes, t64, map, map_off, crpt, ccol, cval, rows, c, pref,
-                                    &ctr->err, s);
+                                    run, &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;
       continue;

@@ -100,7 +100,10 @@ struct Call {
     return h.total_nnz > 0 && (double)intprod >= 1.5 * (double)h.total_nnz;
   }
   // B rows whose loads the staged walk issues ahead: bits 8.. of row_kernel (0 = 4)
-  int rg_depth() const { return (opts.row_kernel >> 8) ? (opts.row_kernel >> 8) : 4; }
+  int rg_depth() const {
+    const int d = (opts.row_kernel >> 8) & 0xff;
+    return d ? d : 4;
+  }
   void mark(int i) {
     if (timing && ev[i]) cudaEventRecord(ev[i], s);
   }

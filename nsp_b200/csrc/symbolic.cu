@@ -147,111 +147,236 @@ __device__ __forceinline__ int sym_map_product(unsigned *table, bool has, unsign
   return idx;
 }
 
+// Row templates (chunk > 1). Rows of structured grids repeat the pattern of
+// their neighbours: the same A row length, the same B row lengths, and
+// product columns that differ from an earlier row's by one shift. Such a row
+// has the earlier row's count and, entry for entry, its map, so it needs no
+// hash probe at all. Each group keeps the last row it hashed whose map was
+// recorded (and that has at most kTplA A entries) as its template: per A
+// entry the start and length of its B row, the row's first column, count,
+// map offset and B column array. A row with the template's A length is
+// compared with it product by product (its columns minus the template's must
+// all equal the difference of the first columns); on a match it takes the
+// template's count and map offset and nothing is hashed or written. Any
+// difference sends the row through the hash walk, which then makes it the
+// template. Groups take their rows in runs of `chunk` consecutive launch rows
+// so that neighbours meet. The numeric pass reads a matched row's map at the
+// template's offset; the walk order, and so every index, is the same.
+constexpr int kTplA = 64;
+constexpr int kMatchRun = 4;  // B rows whose columns a match loads at once
+
+// The scalars of a group's template (shared memory keeps them out of the
+// registers the hash walk needs).
+struct TplHead {
+  int ok, na, mn, nk;
+  unsigned mo;
+  int pad;
+  const int *bcol;
+};
+
+template <int G, int LOG2T>
+struct SymMapCfg {
+  static constexpr int T = 1 << LOG2T;
+  static constexpr int BYTES = T * 4 + kTplA * 8 + 32;  // table, template B rows, TplHead
+  static constexpr int GPC = SymGroupCfg<G, LOG2T>::GPC;
+  static constexpr int THREADS = GPC * G;
+  static constexpr int SMEM = GPC * BYTES;
+};
+
 template <int G, int LOG2T, bool MULTI>
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(256, MULTI ? 4 : 5)
     k_sym_map(const ProdTable<void> src, const int *__restrict__ rows, int count,
               int *__restrict__ row_nz, int *__restrict__ err, unsigned char *__restrict__ map,
               long long bin_off, int stride, unsigned *__restrict__ map_off,
-              int *__restrict__ flags) {
-  using C = SymGroupCfg<G, LOG2T>;
+              int *__restrict__ flags, int chunk) {
+  using C = SymMapCfg<G, LOG2T>;
   extern __shared__ __align__(16) unsigned smem_symm[];
   auto tile = cg::tiled_partition<G>(cg::this_thread_block());
   const int g = threadIdx.x / G;
   const int lane = tile.thread_rank();
   const unsigned below = (1u << lane) - 1u;
-  unsigned *table = smem_symm + g * C::T;
-  for (int r = blockIdx.x * C::GPC + g; r < count; r += gridDim.x * C::GPC) {
-    const int row = rows ? rows[r] : r;
-    uint4 *t4 = reinterpret_cast<uint4 *>(table);
-#pragma unroll 4
-    for (int s = lane; s < C::T / 4; s += G)
-      t4[s] = make_uint4(kMapEmpty, kMapEmpty, kMapEmpty, kMapEmpty);
-    Operands<void> o;
-    const int lr = prod_row<MULTI>(src, row, o);
-    const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
-    // B row bounds of the first G A entries, and the row's first column
-    int bs = 0, be = 0, mn = 0x7fffffff;
-    if (a0 + lane < a1) {
-      const int k = ld_stream(o.acol + a0 + lane);
-      bs = __ldg(o.brpt + k);
-      be = __ldg(o.brpt + k + 1);
-      if (be > bs) mn = __ldg(o.bcol + bs);
-    }
-    for (int j = a0 + G + lane; j < a1; j += G) {
-      const int k = __ldg(o.acol + j);
-      const int s0 = __ldg(o.brpt + k), s1 = __ldg(o.brpt + k + 1);
-      if (s1 > s0) mn = min(mn, __ldg(o.bcol + s0));
-    }
-    mn = cg::reduce(tile, mn, cg::less<int>());
-    tile.sync();  // the table is clear
-    unsigned char *mp = map + bin_off + (size_t)r * stride;
-    int nk = 0;   // distinct columns so far (uniform across the group)
-    int pos = 0;  // map bytes so far, saturated at stride + 1
-    for (int ab = a0; ab < a1; ab += G) {
-      if (ab > a0) {
-        bs = be = 0;
-        if (ab + lane < a1) {
-          const int k = ld_stream(o.acol + ab + lane);
-          bs = __ldg(o.brpt + k);
-          be = __ldg(o.brpt + k + 1);
+  unsigned *table = smem_symm + (size_t)g * (C::BYTES / 4);
+  int2 *tb = reinterpret_cast<int2 *>(table + C::T);  // template: (B row start, length)
+  TplHead *th = reinterpret_cast<TplHead *>(tb + kTplA);
+  const bool use_tpl = chunk > 1;
+  if (lane == 0) th->ok = 0;
+  tile.sync();
+  const int nchunks = (int)(((long long)count + chunk - 1) / chunk);
+  for (int ch = blockIdx.x * C::GPC + g; ch < nchunks; ch += gridDim.x * C::GPC) {
+    const int rend = (int)min((long long)count, (long long)(ch + 1) * chunk);
+    for (int r = ch * chunk; r < rend; ++r) {
+      const int row = rows ? rows[r] : r;
+      Operands<void> o;
+      const int lr = prod_row<MULTI>(src, row, o);
+      const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
+      const int na = a1 - a0;
+      // B row bounds of the first G A entries, and the row's first column
+      int bs = 0, be = 0, mn = 0x7fffffff;
+      if (a0 + lane < a1) {
+        const int k = ld_stream(o.acol + a0 + lane);
+        bs = __ldg(o.brpt + k);
+        be = __ldg(o.brpt + k + 1);
+        if (be > bs) mn = __ldg(o.bcol + bs);
+      }
+      for (int j = a0 + G + lane; j < a1; j += G) {
+        const int k = __ldg(o.acol + j);
+        const int s0 = __ldg(o.brpt + k), s1 = __ldg(o.brpt + k + 1);
+        if (s1 > s0) mn = min(mn, __ldg(o.bcol + s0));
+      }
+      mn = cg::reduce(tile, mn, cg::less<int>());
+      if (th->ok && na == th->na) {
+        // every product's column minus the template's must equal this shift
+        const unsigned delta = (unsigned)mn - (unsigned)th->mn;
+        const int *t_bcol = th->bcol;
+        bool bad = false;
+        int mbs = bs, mbe = be;
+        for (int ab = a0; ab < a1; ab += G) {
+          if (ab > a0) {
+            mbs = mbe = 0;
+            if (ab + lane < a1) {
+              const int k = ld_stream(o.acol + ab + lane);
+              mbs = __ldg(o.brpt + k);
+              mbe = __ldg(o.brpt + k + 1);
+            }
+          }
+          const bool lb = ab + lane < a1 && mbe - mbs != tb[ab - a0 + lane].y;
+          if (tile.any(lb)) {
+            bad = true;
+            break;
+          }
+          const int cnt = min(G, a1 - ab);
+          bool cb = false;
+          int t = 0;
+          // first G entries of kMatchRun B rows at a time (their loads in flight
+          // together), then the rest of any longer B row
+          bool longer = false;
+          for (; t + kMatchRun <= cnt; t += kMatchRun) {
+            unsigned x[kMatchRun], y[kMatchRun];
+#pragma unroll
+            for (int i = 0; i < kMatchRun; ++i) {
+              const int s0 = tile.shfl(mbs, t + i);
+              const int2 tt = tb[ab - a0 + t + i];
+              const bool h = lane < tt.y;
+              longer |= tt.y > G;
+              x[i] = h ? (unsigned)__ldg(o.bcol + s0 + lane) : delta;
+              y[i] = h ? (unsigned)__ldg(t_bcol + tt.x + lane) : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < kMatchRun; ++i) cb |= x[i] - y[i] != delta;
+          }
+          for (; t < cnt; ++t) {
+            const int s0 = tile.shfl(mbs, t);
+            const int2 tt = tb[ab - a0 + t];
+            longer |= tt.y > G;
+            if (lane < tt.y)
+              cb |= (unsigned)__ldg(o.bcol + s0 + lane) - (unsigned)__ldg(t_bcol + tt.x + lane) !=
+                    delta;
+          }
+          if (longer) {  // uniform: tb is read by every lane alike
+            for (t = 0; t < cnt; ++t) {
+              const int s0 = tile.shfl(mbs, t);
+              const int2 tt = tb[ab - a0 + t];
+              for (int e = G + lane; e < tt.y; e += G)
+                cb |= (unsigned)__ldg(o.bcol + s0 + e) - (unsigned)__ldg(t_bcol + tt.x + e) !=
+                      delta;
+            }
+          }
+          if (tile.any(cb)) {
+            bad = true;
+            break;
+          }
+        }
+        if (!bad) {
+          if (lane == 0) {
+            row_nz[row] = th->nk;
+            map_off[row] = th->mo;
+          }
+          continue;
         }
       }
-      const int cnt = min(G, a1 - ab);
-      int t = 0;
-      // quads: one 4-byte word per lane
-      for (; t + 4 <= cnt; t += 4) {
-        int s0[4], len[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          s0[i] = tile.shfl(bs, t + i);
-          len[i] = tile.shfl(be, t + i) - s0[i];
+      // hash walk
+      uint4 *t4 = reinterpret_cast<uint4 *>(table);
+#pragma unroll 4
+      for (int s = lane; s < C::T / 4; s += G)
+        t4[s] = make_uint4(kMapEmpty, kMapEmpty, kMapEmpty, kMapEmpty);
+      tile.sync();  // the table is clear, and the old template is read
+      const bool rec = use_tpl && na <= kTplA;  // this row may become the template
+      unsigned char *mp = map + bin_off + (size_t)r * stride;
+      int nk = 0;   // distinct columns so far (uniform across the group)
+      int pos = 0;  // map bytes so far, saturated at stride + 1
+      for (int ab = a0; ab < a1; ab += G) {
+        if (ab > a0) {
+          bs = be = 0;
+          if (ab + lane < a1) {
+            const int k = ld_stream(o.acol + ab + lane);
+            bs = __ldg(o.brpt + k);
+            be = __ldg(o.brpt + k + 1);
+          }
         }
-        if (!map_quad<G>(len)) break;
-        // the four B rows' columns are loaded before the first insert (the
-        // group barrier of each step would otherwise hold the next load back)
-        unsigned rks[4];
+        if (rec && ab + lane < a1) tb[ab - a0 + lane] = make_int2(bs, be - bs);
+        const int cnt = min(G, a1 - ab);
+        int t = 0;
+        // quads: one 4-byte word per lane
+        for (; t + 4 <= cnt; t += 4) {
+          int s0[4], len[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          rks[i] = lane < len[i] ? (unsigned)(__ldg(o.bcol + s0[i] + lane) - mn) : 0u;
-        unsigned word = 0;
+          for (int i = 0; i < 4; ++i) {
+            s0[i] = tile.shfl(bs, t + i);
+            len[i] = tile.shfl(be, t + i) - s0[i];
+          }
+          if (!map_quad<G>(len)) break;
+          // the four B rows' columns are loaded before the first insert (the
+          // group barrier of each step would otherwise hold the next load back)
+          unsigned rks[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const bool has = lane < len[i];
-          const unsigned rk = rks[i];
-          const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
-          word |= (unsigned)idx << (8 * i);
+          for (int i = 0; i < 4; ++i)
+            rks[i] = lane < len[i] ? (unsigned)(__ldg(o.bcol + s0[i] + lane) - mn) : 0u;
+          unsigned word = 0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const bool has = lane < len[i];
+            const unsigned rk = rks[i];
+            const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
+            word |= (unsigned)idx << (8 * i);
+            tile.sync();  // the next step sees this step's inserts
+          }
+          const int pa = (pos + 3) & ~3;
+          if (pa + 4 * G <= stride) reinterpret_cast<unsigned *>(mp + pa)[lane] = word;
+          pos = min(pa + 4 * G, stride + 1);
+        }
+        // the rest of the chunk: one byte per product
+        for (; t < cnt; ++t) {
+          const int s0 = tile.shfl(bs, t), s1 = tile.shfl(be, t);
+          unsigned char *sp = mp + pos - s0;  // sp[e]: the byte of B entry e
+          const int room = stride - pos;
+          for (int eb = s0; eb < s1; eb += G) {  // uniform trip count across the group
+            const int e = eb + lane;
+            const bool has = e < s1;
+            const unsigned rk = has ? (unsigned)(__ldg(o.bcol + e) - mn) : 0u;
+            const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
+            if (has && e - s0 < room) sp[e] = (unsigned char)idx;
+          }
+          pos = (int)min((long long)pos + (s1 - s0), (long long)stride + 1);
           tile.sync();  // the next step sees this step's inserts
         }
-        const int pa = (pos + 3) & ~3;
-        if (pa + 4 * G <= stride) reinterpret_cast<unsigned *>(mp + pa)[lane] = word;
-        pos = min(pa + 4 * G, stride + 1);
       }
-      // the rest of the chunk: one byte per product
-      for (; t < cnt; ++t) {
-        const int s0 = tile.shfl(bs, t), s1 = tile.shfl(be, t);
-        unsigned char *sp = mp + pos - s0;  // sp[e]: the byte of B entry e
-        const int room = stride - pos;
-        for (int eb = s0; eb < s1; eb += G) {  // uniform trip count across the group
-          const int e = eb + lane;
-          const bool has = e < s1;
-          const unsigned rk = has ? (unsigned)(__ldg(o.bcol + e) - mn) : 0u;
-          const int idx = sym_map_product<G, LOG2T>(table, has, rk, nk, below, tile, err);
-          if (has && e - s0 < room) sp[e] = (unsigned char)idx;
-        }
-        pos = (int)min((long long)pos + (s1 - s0), (long long)stride + 1);
-        tile.sync();  // the next step sees this step's inserts
+      const unsigned mo =
+          pos <= stride ? (unsigned)((bin_off + (long long)r * stride) >> 4) : kNoMap;
+      if (lane == 0) {
+        row_nz[row] = nk;
+        map_off[row] = mo;
+        if (mo == kNoMap) atomicOr(flags, MAP_OVERFLOW);
       }
+      if (use_tpl && lane == 0) {
+        th->ok = rec && mo != kNoMap;
+        th->na = na;
+        th->mn = mn;
+        th->nk = nk;
+        th->mo = mo;
+        th->bcol = o.bcol;
+      }
+      tile.sync();
     }
-    if (lane == 0) {
-      row_nz[row] = nk;
-      if (pos <= stride) {
-        map_off[row] = (unsigned)((bin_off + (long long)r * stride) >> 4);
-      } else {
-        map_off[row] = kNoMap;
-        atomicOr(flags, MAP_OVERFLOW);
-      }
-    }
-    tile.sync();
   }
 }
 
@@ -378,12 +503,14 @@ static cudaError_t sym_group_bin(int bin, const ProdTable<void> &t, const int *r
 template <int G, int LOG2T>
 static cudaError_t run_sym_map(const ProdTable<void> &t, const int *rows, int count,
                                int *row_nz, int *err, const MapArgs &m, cudaStream_t s) {
-  using C = SymGroupCfg<G, LOG2T>;
+  using C = SymMapCfg<G, LOG2T>;
   auto kern = t.prod_of_row ? k_sym_map<G, LOG2T, true> : k_sym_map<G, LOG2T, false>;
-  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM, count, C::GPC);
+  const int chunk = m.chunk > 1 ? m.chunk : 1;
+  const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM,
+                                   (count + chunk - 1) / chunk, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, C::THREADS, C::SMEM, s>>>(t, rows, count, row_nz, err, m.map, m.bin_off, m.stride,
-                                         m.map_off, m.flags);
+                                         m.map_off, m.flags, chunk);
   return cudaGetLastError();
 }
 
