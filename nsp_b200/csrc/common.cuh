@@ -420,4 +420,18 @@ __device__ __forceinline__ int bucket_of(int key, int lo, float scale, int nb) {
   return b < nb - 1 ? b : nb - 1;
 }
 
+// True when B rows k and kt are one run of shifted rows (bit k of bits: B row k is row k-1 moved by one
+// column shift; launch_brow_shift);
+// runs are only followed over 31 rows at most (false beyond).
+__device__ __forceinline__ bool same_run(const unsigned *__restrict__ bits, int k, int kt) {
+  if (k == kt) return true;
+  const int lo = min(k, kt) + 1, hi = max(k, kt);
+  if (hi - lo >= 31) return false;
+  const int wa = lo >> 5, wb = hi >> 5;
+  const unsigned ma = 0xffffffffu << (lo & 31);
+  const unsigned mb = 0xffffffffu >> (31 - (hi & 31));
+  if (wa == wb) return (__ldg(bits + wa) & (ma & mb)) == (ma & mb);
+  return (__ldg(bits + wa) & ma) == ma && (__ldg(bits + wb) & mb) == mb;
+}
+
 }  // namespace nspb

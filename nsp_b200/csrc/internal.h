@@ -117,6 +117,7 @@ struct MapArgs {
   unsigned *map_off = nullptr;   // per global row
   int *flags = nullptr;          // MAP_OVERFLOW
   int chunk = 1;                 // rows a group takes in a run; > 1: row templates
+  const unsigned *bshift = nullptr;  // B row shift bits (launch_brow_shift), or none
 };
 // Row templates of the map symbolic pass: consecutive rows a group takes in a
 // run, and the opts.row_kernel bit that turns templates off.
@@ -193,6 +194,10 @@ cudaError_t launch_symbolic_bin(int bin, int lanes, bool b_sorted, const ProdTab
 // Row-group symbolic bin (bin < kSymGroupBins) that also writes the entry
 // map of each row (B rows strictly increasing; every product's B has at
 // most kMapMaxCols columns).
+// Bit k of bits (nb / 32 + 1 words): B row k is B row k-1 moved by one
+// column shift (same length, same column differences).
+cudaError_t launch_brow_shift(const int *brpt, const int *bcol, int nb, unsigned *bits,
+                              cudaStream_t s);
 cudaError_t launch_symbolic_map(int bin, int lanes, const ProdTable<void> &t, const int *rows,
                                 int count, int *row_nz, int *err, const MapArgs &m,
                                 cudaStream_t s);
@@ -240,16 +245,18 @@ cudaError_t launch_numeric_comp_rg(int bin, int lanes, int tshift, int depth,
 // prefetch_a (single products only): cp.async copies each group's next row's
 // first A entries into shared memory while the current row is computed.
 // run > 1: groups take runs of `run` consecutive rows and reuse the sort of a
-// row for the rows that share its map (row templates of the symbolic pass).
+// row for the rows that share its map (row templates of the symbolic pass) or
+// whose B rows are its B rows moved by one shift (bshift, one product).
 cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
                                const unsigned char *map, const unsigned *map_off,
                                const int *crpt, int *ccol, double *cval, const int *rows,
-                               int count, bool prefetch_a, int run, int *err, cudaStream_t s);
+                               int count, bool prefetch_a, int run, const unsigned *bshift,
+                               int *err, cudaStream_t s);
 // The same for fp32 inputs: rows of at most nmax A entries in fp32 pairs, the
 // others in fp64 from exact products (see launch_numeric_comp_bin).
 cudaError_t launch_numeric_comp_map(int bin, int lanes, const ProdTable<float> &t,
                                     const unsigned char *map, const unsigned *map_off,
                                     const int *crpt, int *ccol, double *cval, const int *rows,
-                                    int count, bool prefetch_a, int run, int nmax, int *redo,
+                                    int count, bool prefetch_a, int run, const unsigned *bshift, int nmax, int *redo,
                                     int *max_deg, int *err, cudaStream_t s);
 }  // namespace nspb

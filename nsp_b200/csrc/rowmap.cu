@@ -65,7 +65,7 @@ template <int G, int LOG2H, bool PREF>
 struct NumMapCfg {
   static constexpr int H = 1 << LOG2H;
   static constexpr int BYTES =
-      (H * 8 + H * 16 + G * 16 + (PREF ? G * 24 : 0) + H * 5 + 15) & ~15;
+      (H * 8 + H * 16 + G * 16 + (PREF ? G * 24 : 0) + G * 12 + H * 5 + 15) & ~15;
   static constexpr int kBySmem = (56 * 1024) / BYTES > 0 ? (56 * 1024) / BYTES : 1;
   static constexpr int GPC = kBySmem < 256 / G ? kBySmem : 256 / G;
   static constexpr int THREADS = GPC * G;
@@ -88,7 +88,8 @@ __global__ void __launch_bounds__(256)
     k_num_map(const ProdTable<VT> src, const unsigned char *__restrict__ map,
               const unsigned *__restrict__ map_off, const int *__restrict__ crpt,
               int *__restrict__ ccol, double *__restrict__ cval, const int *__restrict__ rows,
-              int count, int *__restrict__ err, CompArgs comp, int run) {
+              int count, int *__restrict__ err, CompArgs comp, int run,
+              const unsigned *__restrict__ bshift) {
   static_assert(!(PREF && MULTI), "prefetch serves single products");
   using C = NumMapCfg<G, LOG2H, PREF>;
   constexpr int H = C::H;
@@ -106,12 +107,17 @@ __global__ void __launch_bounds__(256)
   int4 *stage = reinterpret_cast<int4 *>(bkey + H);
   double *avp = reinterpret_cast<double *>(stage + G);  // PREF: [2][G] A values
   int *acp = reinterpret_cast<int *>(avp + 2 * G);      // PREF: [2][G] A columns
-  int *trel = reinterpret_cast<int *>(gb + (size_t)H * 24 + (size_t)G * 16 + (PREF ? G * 24 : 0));
+  // the template row's A entries: B row index, length, first column
+  int *tk = reinterpret_cast<int *>(gb + (size_t)H * 24 + (size_t)G * 16 + (PREF ? G * 24 : 0));
+  int *tl = tk + G;
+  int *tfc = tl + G;
+  int *trel = tfc + G;
   unsigned char *tinv = reinterpret_cast<unsigned char *>(trel + H);
   int4 *c4 = reinterpret_cast<int4 *>(cnt);
-  // the group's template: map offset and entries of the last row it sorted
+  // the group's template: map offset and entries of the last row it sorted,
+  // and the A length of the row tk/tl/tfc hold (-1: none)
   unsigned t_mo = kNoMap;
-  int t_n = -1;
+  int t_n = -1, t_na = -1;
   for (int s = lane; s < H / 4; s += G) c4[s] = make_int4(0, 0, 0, 0);
   tile.sync();
 
@@ -162,12 +168,10 @@ __global__ void __launch_bounds__(256)
     const VT *aval = op.aval, *bval = op.bval;
     const int a0 = op.arpt[lr], a1 = op.arpt[lr + 1];
     const bool pair = COMP && (a1 - a0) <= comp.nmax;
-    // a row of the template: no columns, no first appearances, no sort
-    const bool hit = run > 1 && !pair && mo == t_mo && n == t_n;
-    if (hit) {
-      for (int q = lane; q < n; q += G) vals[q] = 0.0;
-      tile.sync();
-    }
+    // a row of the template: no columns, no first appearances, no sort. It
+    // shares the template's map, or (checked on the first chunk below) its A
+    // entries' B rows are the template's moved by one shift.
+    bool hit = run > 1 && !pair && mo == t_mo && n == t_n;
     int mn = 0x7fffffff, mx = -1;
     int nk = 0;   // distinct columns before the current step (uniform)
     int pos = 0;  // products walked so far (uniform)
@@ -205,8 +209,8 @@ __global__ void __launch_bounds__(256)
     };
     for (int ab = a0; ab < a1; ab += G) {
       const int j = ab + lane;
+      int k = 0, bs = 0, be = 0, fc = 0;
       if (j < a1) {
-        int k;
         double av;
         if (PREF && ab == a0) {
           k = acp[buf * G + lane];
@@ -215,12 +219,40 @@ __global__ void __launch_bounds__(256)
           k = ld_stream(acol + j);
           av = ldv_stream(aval + j);
         }
-        const int bs = __ldg(brpt + k), be = __ldg(brpt + k + 1);
+        bs = __ldg(brpt + k);
+        be = __ldg(brpt + k + 1);
         if (be > bs) {
-          mn = min(mn, __ldg(bcol + bs));
+          fc = __ldg(bcol + bs);
+          mn = min(mn, fc);
           mx = max(mx, __ldg(bcol + be - 1));
         }
         stage[lane] = make_int4(bs, be, __double2loint(av), __double2hiint(av));
+      }
+      if (run > 1 && ab == a0) {
+        const int na0 = a1 - a0;
+        if (!hit && !pair && bshift && n == t_n && na0 <= G && na0 == t_na) {
+          // every B row the row reads is the template's moved by one shift d
+          // (lane 0's B row gives d), so every product column moves by d
+          const int d = fc - tfc[lane < na0 ? lane : 0];
+          const int d0 = tile.shfl(d, 0);
+          bool ok = true;
+          if (lane < na0) {
+            const int len = be - bs;
+            ok = len == tl[lane] && (len == 0 || (d == d0 && same_run(bshift, k, tk[lane])));
+          }
+          hit = tile.shfl(be - bs, 0) > 0 && tile.all(ok);
+        }
+        if (hit) {
+          t_mo = mo;  // the same map bytes as the template's
+          for (int q = lane; q < n; q += G) vals[q] = 0.0;
+        } else {
+          t_na = -1;  // the row that tk/tl/tfc will hold is not sorted yet
+        }
+        if (na0 <= G && lane < na0 && !pair) {
+          tk[lane] = k;
+          tl[lane] = be - bs;
+          tfc[lane] = fc;
+        }
       }
       tile.sync();
       const int na = min(G, a1 - ab);
@@ -390,9 +422,11 @@ __global__ void __launch_bounds__(256)
         tinv[rank] = (unsigned char)q;
       }
     }
-    // the sorted row is the template of the rows that share its map
+    // the sorted row is the template of the rows that share its map or its
+    // shifted pattern
     t_mo = run > 1 && !pair ? mo : kNoMap;
     t_n = n;
+    t_na = run > 1 && !pair && a1 - a0 <= G ? a1 - a0 : -1;
     if (COMP) {
       if (pair) my_max_deg = max(my_max_deg, a1 - a0);
       else ++my_redo;
@@ -412,7 +446,8 @@ template <int G, int LOG2H, typename VT, bool COMP, bool MULTI, bool PREF>
 static cudaError_t run_num_map_k(const ProdTable<VT> &t, const unsigned char *map,
                                  const unsigned *map_off, const int *crpt, int *ccol,
                                  double *cval, const int *rows, int count, int *err,
-                                 CompArgs comp, int run, cudaStream_t s) {
+                                 CompArgs comp, int run, const unsigned *bshift,
+                                 cudaStream_t s) {
   using C = NumMapCfg<G, LOG2H, PREF>;
   auto kern = k_num_map<G, LOG2H, VT, COMP, MULTI, PREF>;
   run = run > 1 ? run : 1;
@@ -420,7 +455,7 @@ static cudaError_t run_num_map_k(const ProdTable<VT> &t, const unsigned char *ma
                                    (count + run - 1) / run, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, C::THREADS, C::SMEM, s>>>(t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                         comp, run);
+                                         comp, run, MULTI ? nullptr : bshift);
   return cudaGetLastError();
 }
 
@@ -428,25 +463,25 @@ template <int G, int LOG2H, typename VT, bool COMP>
 static cudaError_t run_num_map(const ProdTable<VT> &t, const unsigned char *map,
                                const unsigned *map_off, const int *crpt, int *ccol,
                                double *cval, const int *rows, int count, int *err, CompArgs comp,
-                               bool pref, int run, cudaStream_t s) {
+                               bool pref, int run, const unsigned *bshift, cudaStream_t s) {
   if (t.prod_of_row)
     return run_num_map_k<G, LOG2H, VT, COMP, true, false>(t, map, map_off, crpt, ccol, cval,
-                                                          rows, count, err, comp, run, s);
+                                                          rows, count, err, comp, run, bshift, s);
   if (pref)
     return run_num_map_k<G, LOG2H, VT, COMP, false, true>(t, map, map_off, crpt, ccol, cval,
-                                                          rows, count, err, comp, run, s);
+                                                          rows, count, err, comp, run, bshift, s);
   return run_num_map_k<G, LOG2H, VT, COMP, false, false>(t, map, map_off, crpt, ccol, cval, rows,
-                                                         count, err, comp, run, s);
+                                                         count, err, comp, run, bshift, s);
 }
 
 template <int G, typename VT, bool COMP>
 static cudaError_t num_map_bin(int bin, const ProdTable<VT> &t, const unsigned char *map,
                                const unsigned *map_off, const int *crpt, int *ccol,
                                double *cval, const int *rows, int count, int *err, CompArgs comp,
-                               bool pref, int run, cudaStream_t s) {
+                               bool pref, int run, const unsigned *bshift, cudaStream_t s) {
 #define NSPB_NMAP(L2H) \
   run_num_map<G, L2H, VT, COMP>(t, map, map_off, crpt, ccol, cval, rows, count, err, comp, pref, \
-                                run, s)
+                                run, bshift, s)
   switch (bin) {
     case 0: return NSPB_NMAP(4);
     case 1: return NSPB_NMAP(5);
@@ -460,36 +495,38 @@ static cudaError_t num_map_bin(int bin, const ProdTable<VT> &t, const unsigned c
 cudaError_t launch_numeric_map(int bin, int lanes, const ProdTable<double> &t,
                                const unsigned char *map, const unsigned *map_off,
                                const int *crpt, int *ccol, double *cval, const int *rows,
-                               int count, bool prefetch_a, int run, int *err, cudaStream_t s) {
+                               int count, bool prefetch_a, int run, const unsigned *bshift, int *err,
+                               cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin >= kMapNumBins) return cudaErrorInvalidValue;
   const CompArgs none{0, nullptr, nullptr};
   if (lanes == 8)
     return num_map_bin<8, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count,
-                                         err, none, prefetch_a, run, s);
+                                         err, none, prefetch_a, run, bshift, s);
   if (lanes == 16)
     return num_map_bin<16, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count,
-                                          err, none, prefetch_a, run, s);
+                                          err, none, prefetch_a, run, bshift, s);
   return num_map_bin<32, double, false>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                        none, prefetch_a, run, s);
+                                        none, prefetch_a, run, bshift, s);
 }
 
 cudaError_t launch_numeric_comp_map(int bin, int lanes, const ProdTable<float> &t,
                                     const unsigned char *map, const unsigned *map_off,
                                     const int *crpt, int *ccol, double *cval, const int *rows,
-                                    int count, bool prefetch_a, int run, int nmax, int *redo,
+                                    int count, bool prefetch_a, int run, const unsigned *bshift, int nmax,
+                                    int *redo,
                                     int *max_deg, int *err, cudaStream_t s) {
   if (count <= 0) return cudaSuccess;
   if (bin >= kMapNumBins) return cudaErrorInvalidValue;
   const CompArgs comp{nmax, redo, max_deg};
   if (lanes == 8)
     return num_map_bin<8, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                       comp, prefetch_a, run, s);
+                                       comp, prefetch_a, run, bshift, s);
   if (lanes == 16)
     return num_map_bin<16, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                        comp, prefetch_a, run, s);
+                                        comp, prefetch_a, run, bshift, s);
   return num_map_bin<32, float, true>(bin, t, map, map_off, crpt, ccol, cval, rows, count, err,
-                                      comp, prefetch_a, run, s);
+                                      comp, prefetch_a, run, bshift, s);
 }
 
 }  // namespace nspb

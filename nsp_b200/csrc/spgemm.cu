@@ -332,12 +332,23 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
       total += (long long)h.sym_counts[b] * map_stride[b];
     }
     const size_t head = align256((size_t)n * 4);
+    // row templates of one product check B rows by their shift bits
+    const bool shift_bits = !(opts.row_kernel & kNoRowTemplates) && !table;
+    const size_t bits = shift_bits ? align256(((size_t)B.nrows / 32 + 1) * 4) : 0;
     // at most an eighth of the device's memory (C is allocated after this phase)
-    if ((head + (size_t)total) * 8 <= dev_info().total_mem &&
-        scratch_alloc(&map_block, head + (size_t)total, s) == NSPB_OK) {
+    if ((head + bits + (size_t)total) * 8 <= dev_info().total_mem &&
+        scratch_alloc(&map_block, head + bits + (size_t)total, s) == NSPB_OK) {
       map_off = static_cast<unsigned *>(map_block);
-      map = static_cast<unsigned char *>(map_block) + head;
+      bshift = shift_bits ? reinterpret_cast<unsigned *>(static_cast<unsigned char *>(map_block) +
+                                                         head)
+                          : nullptr;
+      map = static_cast<unsigned char *>(map_block) + head + bits;
       use_map = true;
+      if (bshift) {
+        if ((e = launch_brow_shift(B.rpt, B.col, B.nrows, bshift, s)) != cudaSuccess)
+          return cuda_fail(e);
+        ++launches;
+      }
     }
   }
   mark(2);
@@ -359,7 +370,8 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
       m.stride = map_stride[b];
       m.map_off = map_off;
       m.flags = &ctr->flags;
-      m.chunk = opts.row_kernel & kNoRowTemplates ? 1 : kTemplateRun;
+      m.chunk = template_run();
+      m.bshift = bshift;
       e = launch_symbolic_map(b, lanes, structure_of(t64), rows, c, row_nz, &ctr->err, m, s);
     } else {
       e = launch_symbolic_bin(b, lanes, b_sorted, structure_of(t64), info, rows, c, row_nz,
@@ -382,6 +394,7 @@ int Call::symbolic(int *crpt, int64_t *nnz_out) {
     map_block = nullptr;
     map = nullptr;
     map_off = nullptr;
+    bshift = nullptr;
   }
   if (h.total_nnz > INT32_MAX) return NSPB_ERR_OVERFLOW;
   *nnz_out = h.total_nnz;
@@ -420,12 +433,12 @@ int Call::numeric(const int *crpt, int *ccol, double *cval) {
       // Laplacian 128^3: numeric 1.47 -> 1.16 ms) and costs on long ones
       // (27-point stencil 128^3: 6.63 -> 7.42 ms, L1 data pipe saturated)
       const bool pref = !table && a_nnz <= 12LL * n;
-      const int run = opts.row_kernel & kNoRowTemplates ? 1 : kTemplateRun;
+      const int run = template_run();
       e = comp ? launch_numeric_comp_map(b, lanes, t32, map, map_off, crpt, ccol, cval, rows, c,
-                                         pref, run, nmax, &ctr->redo_count, &ctr->max_comp_deg,
-                                         &ctr->err, s)
+                                         pref, run, bshift, nmax, &ctr->redo_count,
+                                         &ctr->max_comp_deg, &ctr->err, s)
                : launch_numeric_map(b, lanes, t64, map, map_off, crpt, ccol, cval, rows, c, pref,
-                                    run, &ctr->err, s);
+                                    run, bshift, &ctr->err, s);
       if (e != cudaSuccess) return cuda_fail(e);
       ++launches;
       continue;

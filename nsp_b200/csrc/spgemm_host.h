@@ -80,9 +80,10 @@ struct Call {
   // whose numeric phase runs in another call, or that may not allocate.
   bool allow_map = true;
   bool use_map = false;
-  void *map_block = nullptr;   // pool block: map_off (n entries), then the map
+  void *map_block = nullptr;   // pool block: map_off (n entries), B row shift bits, the map
   unsigned char *map = nullptr;
   unsigned *map_off = nullptr;
+  unsigned *bshift = nullptr;  // B row shift bits for the row templates (one product)
   bool map_wanted() const;
   // opts.timing: events around rowinfo, symbolic, scan, numeric
   cudaEvent_t ev[8] = {};
@@ -100,6 +101,13 @@ struct Call {
     return h.total_nnz > 0 && (double)intprod >= 1.5 * (double)h.total_nnz;
   }
   // B rows whose loads the staged walk issues ahead: bits 8.. of row_kernel (0 = 4)
+  // Rows a group takes in a run on the entry-map path (row templates): bits
+  // 20..27 of row_kernel (0 = kTemplateRun); 1 with templates turned off.
+  int template_run() const {
+    if (opts.row_kernel & kNoRowTemplates) return 1;
+    const int r = (opts.row_kernel >> 20) & 0xff;
+    return r ? r : kTemplateRun;
+  }
   int rg_depth() const {
     const int d = (opts.row_kernel >> 8) & 0xff;
     return d ? d : 4;

@@ -165,6 +165,36 @@ __device__ __forceinline__ int sym_map_product(unsigned *table, bool has, unsign
 constexpr int kTplA = 64;
 constexpr int kMatchRun = 4;  // B rows whose columns a match loads at once
 
+// B row shifts: bit k of bshift is set when B row k holds as many entries as
+// row k-1 and every column of row k minus its first column equals the same
+// difference in row k-1 (row k is row k-1 moved by one column shift). Rows
+// k' < k lie in one run of such rows when bits k'+1..k are all set, and then
+// row k is row k' moved by bcol[first of k] - bcol[first of k'].
+__global__ void __launch_bounds__(256)
+    k_brow_shift(const int *__restrict__ brpt, const int *__restrict__ bcol, int nb,
+                 unsigned *__restrict__ bits) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool same = false;
+  if (k > 0 && k < nb) {
+    const int s0 = __ldg(brpt + k - 1), s1 = __ldg(brpt + k), e1 = __ldg(brpt + k + 1);
+    const int len = e1 - s1;
+    same = len == s1 - s0;
+    if (same && len > 0) {
+      const int d = __ldg(bcol + s1) - __ldg(bcol + s0);
+      for (int e = 1; e < len && same; ++e) same = __ldg(bcol + s1 + e) - __ldg(bcol + s0 + e) == d;
+    }
+  }
+  const unsigned w = __ballot_sync(0xffffffffu, same);
+  if ((threadIdx.x & 31) == 0 && k < nb) bits[k >> 5] = w;
+}
+
+cudaError_t launch_brow_shift(const int *brpt, const int *bcol, int nb, unsigned *bits,
+                              cudaStream_t s) {
+  if (nb <= 0) return cudaSuccess;
+  k_brow_shift<<<(nb + 255) / 256, 256, 0, s>>>(brpt, bcol, nb, bits);
+  return cudaGetLastError();
+}
+
 // The scalars of a group's template (shared memory keeps them out of the
 // registers the hash walk needs).
 struct TplHead {
@@ -177,7 +207,7 @@ struct TplHead {
 template <int G, int LOG2T>
 struct SymMapCfg {
   static constexpr int T = 1 << LOG2T;
-  static constexpr int BYTES = T * 4 + kTplA * 8 + 32;  // table, template B rows, TplHead
+  static constexpr int BYTES = T * 4 + kTplA * 16 + 32;  // table, template B rows, TplHead
   static constexpr int GPC = SymGroupCfg<G, LOG2T>::GPC;
   static constexpr int THREADS = GPC * G;
   static constexpr int SMEM = GPC * BYTES;
@@ -188,7 +218,7 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
     k_sym_map(const ProdTable<void> src, const int *__restrict__ rows, int count,
               int *__restrict__ row_nz, int *__restrict__ err, unsigned char *__restrict__ map,
               long long bin_off, int stride, unsigned *__restrict__ map_off,
-              int *__restrict__ flags, int chunk) {
+              int *__restrict__ flags, int chunk, const unsigned *__restrict__ bshift) {
   using C = SymMapCfg<G, LOG2T>;
   extern __shared__ __align__(16) unsigned smem_symm[];
   auto tile = cg::tiled_partition<G>(cg::this_thread_block());
@@ -196,7 +226,8 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
   const int lane = tile.thread_rank();
   const unsigned below = (1u << lane) - 1u;
   unsigned *table = smem_symm + (size_t)g * (C::BYTES / 4);
-  int2 *tb = reinterpret_cast<int2 *>(table + C::T);  // template: (B row start, length)
+  // template, per A entry: B row start, length, B row index, first column
+  int4 *tb = reinterpret_cast<int4 *>(table + C::T);
   TplHead *th = reinterpret_cast<TplHead *>(tb + kTplA);
   const bool use_tpl = chunk > 1;
   if (lane == 0) th->ok = 0;
@@ -211,12 +242,12 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
       const int a0 = o.arpt[lr], a1 = o.arpt[lr + 1];
       const int na = a1 - a0;
       // B row bounds of the first G A entries, and the row's first column
-      int bs = 0, be = 0, mn = 0x7fffffff;
+      int bs = 0, be = 0, mn = 0x7fffffff, k0 = 0, fc0 = 0;
       if (a0 + lane < a1) {
-        const int k = ld_stream(o.acol + a0 + lane);
-        bs = __ldg(o.brpt + k);
-        be = __ldg(o.brpt + k + 1);
-        if (be > bs) mn = __ldg(o.bcol + bs);
+        k0 = ld_stream(o.acol + a0 + lane);
+        bs = __ldg(o.brpt + k0);
+        be = __ldg(o.brpt + k0 + 1);
+        if (be > bs) mn = fc0 = __ldg(o.bcol + bs);
       }
       for (int j = a0 + G + lane; j < a1; j += G) {
         const int k = __ldg(o.acol + j);
@@ -224,8 +255,24 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
         if (s1 > s0) mn = min(mn, __ldg(o.bcol + s0));
       }
       mn = cg::reduce(tile, mn, cg::less<int>());
+      bool hit = false;
       if (th->ok && na == th->na) {
         // every product's column minus the template's must equal this shift
+        const unsigned delta = (unsigned)mn - (unsigned)th->mn;
+        // one chunk of A entries whose B rows each lie in one run of shifted
+        // rows with the template's, moved by delta: every product column is
+        // the template's plus delta, with no column compared
+        if (bshift && na <= G) {
+          bool ok = true;
+          if (lane < na) {
+            const int4 tt = tb[lane];
+            ok = be - bs == tt.y &&
+                 (tt.y == 0 || ((unsigned)fc0 - (unsigned)tt.w == delta && same_run(bshift, k0, tt.z)));
+          }
+          hit = tile.all(ok);
+        }
+      }
+      if (!hit && th->ok && na == th->na) {
         const unsigned delta = (unsigned)mn - (unsigned)th->mn;
         const int *t_bcol = th->bcol;
         bool bad = false;
@@ -255,7 +302,7 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
 #pragma unroll
             for (int i = 0; i < kMatchRun; ++i) {
               const int s0 = tile.shfl(mbs, t + i);
-              const int2 tt = tb[ab - a0 + t + i];
+              const int4 tt = tb[ab - a0 + t + i];
               const bool h = lane < tt.y;
               longer |= tt.y > G;
               x[i] = h ? (unsigned)__ldg(o.bcol + s0 + lane) : delta;
@@ -266,7 +313,7 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
           }
           for (; t < cnt; ++t) {
             const int s0 = tile.shfl(mbs, t);
-            const int2 tt = tb[ab - a0 + t];
+            const int4 tt = tb[ab - a0 + t];
             longer |= tt.y > G;
             if (lane < tt.y)
               cb |= (unsigned)__ldg(o.bcol + s0 + lane) - (unsigned)__ldg(t_bcol + tt.x + lane) !=
@@ -275,7 +322,7 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
           if (longer) {  // uniform: tb is read by every lane alike
             for (t = 0; t < cnt; ++t) {
               const int s0 = tile.shfl(mbs, t);
-              const int2 tt = tb[ab - a0 + t];
+              const int4 tt = tb[ab - a0 + t];
               for (int e = G + lane; e < tt.y; e += G)
                 cb |= (unsigned)__ldg(o.bcol + s0 + e) - (unsigned)__ldg(t_bcol + tt.x + e) !=
                       delta;
@@ -286,13 +333,25 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
             break;
           }
         }
-        if (!bad) {
-          if (lane == 0) {
-            row_nz[row] = th->nk;
-            map_off[row] = th->mo;
-          }
-          continue;
+        hit = !bad;
+      }
+      if (hit) {
+        if (lane == 0) {
+          row_nz[row] = th->nk;
+          map_off[row] = th->mo;
         }
+        if (bshift && na <= G) {
+          // the row stands in for the template from here on (same count and
+          // map): the next rows' shift check then spans a few rows, not the
+          // distance back to the row that was hashed
+          if (lane < na) tb[lane] = make_int4(bs, be - bs, k0, fc0);
+          if (lane == 0) {
+            th->mn = mn;
+            th->bcol = o.bcol;
+          }
+          tile.sync();
+        }
+        continue;
       }
       // hash walk
       uint4 *t4 = reinterpret_cast<uint4 *>(table);
@@ -313,7 +372,11 @@ __global__ void __launch_bounds__(256, MULTI ? 4 : 5)
             be = __ldg(o.brpt + k + 1);
           }
         }
-        if (rec && ab + lane < a1) tb[ab - a0 + lane] = make_int2(bs, be - bs);
+        if (rec && ab + lane < a1) {
+          // the first chunk keeps its B row indices and first columns (k0, fc0)
+          // for the shift check; later chunks are only ever compared column by column
+          tb[ab - a0 + lane] = ab == a0 ? make_int4(bs, be - bs, k0, fc0) : make_int4(bs, be - bs, 0, 0);
+        }
         const int cnt = min(G, a1 - ab);
         int t = 0;
         // quads: one 4-byte word per lane
@@ -510,7 +573,7 @@ static cudaError_t run_sym_map(const ProdTable<void> &t, const int *rows, int co
                                    (count + chunk - 1) / chunk, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;
   kern<<<grid, C::THREADS, C::SMEM, s>>>(t, rows, count, row_nz, err, m.map, m.bin_off, m.stride,
-                                         m.map_off, m.flags, chunk);
+                                         m.map_off, m.flags, chunk, t.prod_of_row ? nullptr : m.bshift);
   return cudaGetLastError();
 }
 

@@ -49,8 +49,8 @@ def product(A, B, **kw):
     return C.to_host(), st
 
 
-def check(A, B, **kw):
-    got, st = product(A, B, row_kernel=7, **kw)
+def check(A, B, row_kernel_bits=0, **kw):
+    got, st = product(A, B, row_kernel=7 | row_kernel_bits, **kw)
     rp, col, val = oracle.spgemm(A, B)
     assert_same_structure(got.rowptr, got.col, rp, col)
     assert_bitwise(got.val, val)
@@ -66,6 +66,14 @@ def test_stencil27(cuda, lanes):
     # lanes 8 and 16: B rows of 27 entries are longer than the group
     A = nb.gen.stencil(18, npts=27)
     check(A, A, group_lanes=lanes)
+
+
+@pytest.mark.parametrize("run", [2, 5, 64])
+def test_run_lengths(cuda, run):
+    # rows a group takes in a run (opts.row_kernel bits 20..27)
+    A = nb.gen.stencil(15, npts=27)
+    P = perturb(A, 0.02, seed=17)
+    check(P, P, row_kernel_bits=run << 20)
 
 
 def test_stencil7(cuda):
