@@ -117,6 +117,7 @@ struct MapArgs {
   unsigned *map_off = nullptr;   // per global row
   int *flags = nullptr;          // MAP_OVERFLOW
   int chunk = 1;                 // rows a group takes in a run; > 1: row templates
+                                 // (negative: exactly -chunk, see template_chunk)
   const unsigned *bshift = nullptr;  // B row shift bits (launch_brow_shift), or none
 };
 // Row templates of the map symbolic pass: consecutive rows a group takes in a

@@ -70,4 +70,19 @@ inline int persistent_grid(const void *func, int threads, int smem, long long it
   return (int)(need < cap ? need : cap);
 }
 
+// Rows a row group takes in a run (row templates), at most `run`: a bin too
+// small to give every resident group `run` rows gets shorter runs (1: no
+// templates), so that its rows still spread over all the groups instead of
+// queueing behind a few. A negative run is the caller's own (-run rows, as
+// given).
+inline int template_chunk(int run, long long count, const void *func, int threads, int smem,
+                          int per_cta) {
+  if (run < 0) return -run;
+  if (run <= 1) return 1;
+  const int occ = resident_ctas(func, threads, smem);
+  const long long groups = (long long)(occ > 0 ? occ : 1) * dev_info().sms * per_cta;
+  const long long fit = count / groups;
+  return (int)(fit < run ? (fit > 1 ? fit : 1) : run);
+}
+
 }  // namespace nspb

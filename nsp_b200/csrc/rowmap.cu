@@ -450,7 +450,7 @@ static cudaError_t run_num_map_k(const ProdTable<VT> &t, const unsigned char *ma
                                  cudaStream_t s) {
   using C = NumMapCfg<G, LOG2H, PREF>;
   auto kern = k_num_map<G, LOG2H, VT, COMP, MULTI, PREF>;
-  run = run > 1 ? run : 1;
+  run = template_chunk(run, count, (const void *)kern, C::THREADS, C::SMEM, C::GPC);
   const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM,
                                    (count + run - 1) / run, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;

@@ -102,11 +102,13 @@ struct Call {
   }
   // B rows whose loads the staged walk issues ahead: bits 8.. of row_kernel (0 = 4)
   // Rows a group takes in a run on the entry-map path (row templates): bits
-  // 20..27 of row_kernel (0 = kTemplateRun); 1 with templates turned off.
+  // 20..27 of row_kernel, taken as given (returned negative, see
+  // template_chunk), or kTemplateRun, shortened for small bins; 1 with
+  // templates turned off.
   int template_run() const {
     if (opts.row_kernel & kNoRowTemplates) return 1;
     const int r = (opts.row_kernel >> 20) & 0xff;
-    return r ? r : kTemplateRun;
+    return r ? -r : kTemplateRun;
   }
   int rg_depth() const {
     const int d = (opts.row_kernel >> 8) & 0xff;

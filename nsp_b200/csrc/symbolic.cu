@@ -568,7 +568,8 @@ static cudaError_t run_sym_map(const ProdTable<void> &t, const int *rows, int co
                                int *row_nz, int *err, const MapArgs &m, cudaStream_t s) {
   using C = SymMapCfg<G, LOG2T>;
   auto kern = t.prod_of_row ? k_sym_map<G, LOG2T, true> : k_sym_map<G, LOG2T, false>;
-  const int chunk = m.chunk > 1 ? m.chunk : 1;
+  const int chunk = template_chunk(m.chunk, count, (const void *)kern, C::THREADS, C::SMEM,
+                                   C::GPC);
   const int grid = persistent_grid((const void *)kern, C::THREADS, C::SMEM,
                                    (count + chunk - 1) / chunk, C::GPC);
   if (grid <= 0) return cudaErrorInvalidConfiguration;

@@ -18,6 +18,10 @@ from conftest import assert_bitwise, assert_same_structure
 pytestmark = pytest.mark.gpu
 
 NO_TEMPLATES = 0x10000  # opts.row_kernel bit: row templates off
+# opts.row_kernel bits 20..27: rows a group takes in a run, exactly as given.
+# The automatic run is shortened for launches with few rows per resident
+# group (1: no templates), which these small inputs would be.
+RUN16 = 16 << 20
 
 
 def perturb(M: HostCSR, frac: float, seed: int) -> HostCSR:
@@ -49,7 +53,7 @@ def product(A, B, **kw):
     return C.to_host(), st
 
 
-def check(A, B, row_kernel_bits=0, **kw):
+def check(A, B, row_kernel_bits=RUN16, **kw):
     got, st = product(A, B, row_kernel=7 | row_kernel_bits, **kw)
     rp, col, val = oracle.spgemm(A, B)
     assert_same_structure(got.rowptr, got.col, rp, col)
@@ -74,6 +78,14 @@ def test_run_lengths(cuda, run):
     A = nb.gen.stencil(15, npts=27)
     P = perturb(A, 0.02, seed=17)
     check(P, P, row_kernel_bits=run << 20)
+
+
+@pytest.mark.parametrize("L", [12, 40])
+def test_automatic_run(cuda, L):
+    # the library's own run length: 12^3 gives every group about one row (no
+    # templates), 40^3 about ten
+    A = nb.gen.stencil(L, npts=27)
+    check(A, A, row_kernel_bits=0)
 
 
 def test_stencil7(cuda):
@@ -112,7 +124,8 @@ def test_shifted_values_differ(cuda):
 def test_batched_identical_products(cuda, monkeypatch):
     # rows of one launch come from two products with their own B arrays: a
     # template found in one product serves rows of the other
-    monkeypatch.setenv("NSPB_ROW_KERNEL", "7")  # entry maps (the batched entry's opts)
+    # entry maps and runs of 16 rows (the batched entry takes its opts from here)
+    monkeypatch.setenv("NSPB_ROW_KERNEL", str(7 | RUN16))
     A = nb.gen.stencil(12, npts=27)
     A2 = HostCSR(A.nrows, A.ncols, A.rowptr.copy(), A.col.copy(), A.val * 0.5)
     dA, dA2 = A.to_device(), A2.to_device()
