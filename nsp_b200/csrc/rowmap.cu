@@ -235,12 +235,25 @@ __global__ void __launch_bounds__(256)
           // (lane 0's B row gives d), so every product column moves by d
           const int d = fc - tfc[lane < na0 ? lane : 0];
           const int d0 = tile.shfl(d, 0);
-          bool ok = true;
-          if (lane < na0) {
-            const int len = be - bs;
-            ok = len == tl[lane] && (len == 0 || (d == d0 && same_run(bshift, k, tk[lane])));
+          const int len = lane < na0 ? be - bs : 0;
+          const bool lens = lane >= na0 || len == tl[lane];
+          const bool ok =
+              lens && (lane >= na0 || len == 0 || (d == d0 && same_run(bshift, k, tk[lane])));
+          const bool based = tile.shfl(be - bs, 0) > 0;
+          hit = based && tile.all(ok);
+          if (!hit && based && tile.all(lens)) {
+            // the shift bits cannot decide (the first row of a run is far from
+            // the row sorted last): compare the columns themselves
+            const int tbs = len > 0 ? __ldg(brpt + tk[lane]) : 0;
+            bool diff = false;
+            for (int t = 0; t < na0; ++t) {
+              const int s0 = tile.shfl(bs, t), s1 = tile.shfl(tbs, t), ln = tile.shfl(len, t);
+              for (int e = lane; e < ln; e += G)
+                diff |= (unsigned)__ldg(bcol + s0 + e) - (unsigned)__ldg(bcol + s1 + e) !=
+                        (unsigned)d0;
+            }
+            hit = !tile.any(diff);
           }
-          hit = tile.shfl(be - bs, 0) > 0 && tile.all(ok);
         }
         if (hit) {
           t_mo = mo;  // the same map bytes as the template's
