@@ -128,7 +128,15 @@ typedef struct {
                             table (0 takes maps when the B rows read fill
                             3/4 of the row groups' lanes on average; maps
                             need one-call products, sorted B rows, no row of
-                            more than 3072 products, < 2^24 columns)        */
+                            more than 3072 products, < 2^24 columns).
+                            With maps, rows that repeat a neighbour's
+                            pattern (the same A and B row lengths, every
+                            product column moved by one shift) reuse its
+                            count, map and sort (row templates): bit 16
+                            (0x10000) turns them off; bits 8..15: B rows
+                            the staged walk loads ahead (0 = 4); bits
+                            20..27: rows a row group takes in a run (0 =
+                            16, shorter for small bins)                    */
   int32_t sym_fill_pct;  /* symbolic bin thresholds: a row goes to the bin
                             whose table (32 << b slots) it fills to at most
                             this percentage at its upper bound of distinct
