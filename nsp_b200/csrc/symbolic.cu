@@ -151,17 +151,24 @@ __device__ __forceinline__ int sym_map_product(unsigned *table, bool has, unsign
 // their neighbours: the same A row length, the same B row lengths, and
 // product columns that differ from an earlier row's by one shift. Such a row
 // has the earlier row's count and, entry for entry, its map, so it needs no
-// hash probe at all. Each group keeps the last row it hashed whose map was
-// recorded (and that has at most kTplA A entries) as its template: per A
-// entry the start and length of its B row, the row's first column, count,
-// map offset and B column array. A row with the template's A length is
-// compared with it product by product (its columns minus the template's must
-// all equal the difference of the first columns); on a match it takes the
-// template's count and map offset and nothing is hashed or written. Any
-// difference sends the row through the hash walk, which then makes it the
-// template. Groups take their rows in runs of `chunk` consecutive launch rows
-// so that neighbours meet. The numeric pass reads a matched row's map at the
-// template's offset; the walk order, and so every index, is the same.
+// hash probe at all. Each group keeps a template: per A entry the start,
+// length, index and first column of its B row, and the row's first column,
+// count, map offset and B column array. It is the last row the group hashed
+// whose map was recorded (and that has at most kTplA A entries), moved on to
+// every later row that matched it. A row with the template's A length
+// matches when
+//  - (one chunk of A entries, one product) each B row has the template's
+//    length and lies in one run of shifted B rows with the template's (the
+//    B row shift bits below), moved by the same shift as the row's first
+//    column: then every product column is the template's plus that shift; or
+//  - else, its columns minus the template's, product by product, all equal
+//    the difference of the first columns.
+// A matching row takes the template's count and map offset and nothing is
+// hashed or written. Any difference sends the row through the hash walk,
+// which then makes it the template. Groups take their rows in runs of `chunk`
+// consecutive launch rows so that neighbours meet. The numeric pass reads a
+// matched row's map at the template's offset; the walk order, and so every
+// index, is the same.
 constexpr int kTplA = 64;
 constexpr int kMatchRun = 4;  // B rows whose columns a match loads at once
 
