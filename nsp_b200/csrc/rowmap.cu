@@ -52,11 +52,18 @@ __device__ __forceinline__ int map_bucket(unsigned r, unsigned mul, int nb) {
 // column) and tinv[H] (the entry index of each rank).
 //
 // Row templates (run > 1): groups take their rows in runs of `run`
-// consecutive launch rows. A row whose map offset equals the offset of the
-// last row the group sorted has that row's pattern (the symbolic pass gave
-// both rows one map only after checking every product column against the
-// template's, shift for shift), so the sort's outcome carries over: the
-// group adds the products into zeroed values at their indices, with no
+// consecutive launch rows and keep the last row they sorted as a template
+// (its map offset, entry count, per A entry the B row index, length and first
+// column, and the outcome of its sort). A row has the template's pattern, and
+// so its map bytes and its sorted order, when
+//  - its map offset is the template's (the symbolic pass gave both rows one
+//    map only after checking that every product column is one shift of the
+//    template's), or
+//  - (one chunk of A entries, one product) each B row has the template's
+//    length and lies in one run of shifted B rows with the template's (B row
+//    shift bits), all moved by one shift; or, where the bits cannot decide,
+//    its B rows' columns minus the template's all equal that shift.
+// Such a row adds the products into zeroed values at their indices, with no
 // column loads, no first-appearance tracking and no sort, and stores entry
 // tinv[q] at rank q with column trel[q] + the row's first column. Sums run in
 // the same order from the same zero, so the values are bit for bit those of
