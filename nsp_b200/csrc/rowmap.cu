@@ -48,8 +48,9 @@ __device__ __forceinline__ int map_bucket(unsigned r, unsigned mul, int nb) {
 // Per group: vals[H] fp64, keys[H], info[H] (index inside the bucket), cnt[H],
 // bkey[H] (keys in bucket order), stage[G]; with PREF two buffers of G A
 // entries (values, then columns) that cp.async fills for the group's next row;
-// then the row template: trel[H] (its columns in order, less its first
-// column) and tinv[H] (the entry index of each rank).
+// then the row template: tk/tl/tfc[G] (B row index, length and first column
+// of each A entry), trel[H] (its columns in order, less its first column) and
+// tinv[H] (the entry index of each rank).
 //
 // Row templates (run > 1): groups take their rows in runs of `run`
 // consecutive launch rows and keep the last row they sorted as a template
